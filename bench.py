@@ -1,0 +1,496 @@
+#!/usr/bin/env python
+"""Benchmark: delay-and-sum throughput in points/s (voxel x channel x transmit x frame).
+
+One step = one complete beamforming job of the chosen workload (default: 75-transmit
+coherent compounding, 128 elements, 512x512 grid, 3328 complex64 IQ samples, quadratic
+interpolation, f# 1.75) with every input already in HBM.  Prints ONE JSON line on rank 0.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--workload compound|doppler|plain2d|volume3d|volume3d16] [--storage c64|cf16|...]
+
+--impl reference times mach's own CUDA kernel (built from its unmodified source into
+oracle/_ref) on the same inputs, driven as mach drives it: one launch and one
+cudaDeviceSynchronize per transmit into a zeroed output.
+
+Multi-GPU (torchrun): every rank runs its own full job on its own GPU (voxels and jobs are
+independent; there is no data exchange), so scaling is weak; the time is the max over ranks.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+import warnings
+from datetime import timedelta
+from pathlib import Path
+
+import numpy as np
+import torch
+
+REPO = Path(__file__).resolve().parent
+sys.path.insert(0, str(REPO))
+
+METRIC = "points/s (voxel*channel*transmit*frame)"
+
+WORKLOAD_DESC = {
+    "compound": "75 plane waves -16..16 deg, 128-el linear array, 512x512 grid (40x50 mm), 3328 IQ samples, "
+    "quadratic interpolation, f# 1.75, Tukey 0.5",
+    "doppler": "5 plane waves x 200 frames, 128 el, 256x256 grid, 1024 IQ samples, linear, f# 1.0",
+    "plain2d": "single 0 deg plane wave, 128 el, 256x256 grid, 2048 float32 RF samples, linear, Hann f# 1.5",
+    "volume3d": "9 diverging waves, 32x32 matrix array, 128^3 grid, 2048 int16 RF samples, 1 frame, linear, f# 1.0",
+    "volume3d16": "9 diverging waves, 32x32 matrix array, 128^3 grid, 2048 int16 RF samples, 16 frames, linear, f# 1.0",
+}
+
+
+def parse_args():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--workload", choices=sorted(WORKLOAD_DESC), default="compound")
+    p.add_argument("--storage", default=None, help="channel storage (default: the workload's own)")
+    p.add_argument("--cpu-seconds", type=float, default=10.0, help="target CPU time of the cpu_baseline sample")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    return p.parse_args()
+
+
+# ----------------------------------------------------------------------------- plumbing
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        torch.distributed.init_process_group("nccl", timeout=timedelta(seconds=180), device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        torch.distributed.barrier()
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines: list[str] = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.gpu)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peak_hbm():
+    path = REPO / "MEASURED_PEAKS.json"
+    if path.exists():
+        return float(json.loads(path.read_text())["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profiled_traffic(key: str):
+    path = REPO / "profiles" / "dram_traffic.json"
+    if path.exists():
+        table = json.loads(path.read_text())
+        entry = table.get(key)
+        if entry:
+            return entry.get("bytes_per_launch")
+    return None
+
+
+# ----------------------------------------------------------------------------- workloads
+
+
+def make_workload(name: str):
+    from mach_b200 import workloads as W
+
+    if name == "volume3d":
+        return W.volume3d(n_frames=1, device="cuda")
+    if name == "volume3d16":
+        return W.volume3d(n_frames=16, device="cuda")
+    return W.CONFIGS[name](device="cuda")
+
+
+def storage_channel(w, storage):
+    from mach_b200 import workloads as W
+
+    return W.to_storage(w, storage).contiguous()
+
+
+def algorithmic_bytes(w, storage) -> int:
+    esz = {"f32": 4, "c64": 8, "f16": 2, "cf16": 4, "bf16": 2, "cbf16": 4, "i16": 2, "ci16": 4}[storage]
+    out_esz = 8 if storage in ("c64", "cf16", "cbf16", "ci16") else 4
+    return (w.n_tx * w.n_rx * w.n_samples * w.n_frames * esz + w.n_tx * w.n_vox * 4 + w.n_vox * 12 + w.n_rx * 12
+            + w.n_vox * w.n_frames * out_esz)
+
+
+# ----------------------------------------------------------------------------- our arm
+
+
+def run_ours(args, world, rank, local):
+    from mach_b200 import _cuda_impl, _dlpack, experimental
+
+    w = make_workload(args.workload)
+    storage = args.storage or w.storage
+    ch = storage_channel(w, storage)
+    dev = torch.device("cuda", local)
+    rx = torch.as_tensor(w.rx_coords_m, device=dev)
+    scan = torch.as_tensor(w.scan_coords_m, device=dev)
+    arr = torch.as_tensor(w.tx_wave_arrivals_s, device=dev)
+    is_c = storage in ("c64", "cf16", "cbf16", "ci16")
+    out = torch.zeros((w.n_vox, w.n_frames), dtype=torch.complex64 if is_c else torch.float32, device=dev)
+    v_ch, v_rx, v_scan, v_arr, v_out = (_dlpack.view(t) for t in (ch, rx, scan, arr, out))
+    stream = torch.cuda.current_stream(dev)
+    p = w.params
+    common = dict(n_tx=w.n_tx, n_rx=w.n_rx, n_samples=w.n_samples, n_vox=w.n_vox, n_frames=w.n_frames,
+                  f_number=p["f_number"], rx_start_s=p["rx_start_s"], sampling_freq_hz=p["sampling_freq_hz"],
+                  sound_speed_m_s=p["sound_speed_m_s"], modulation_freq_hz=p["modulation_freq_hz"],
+                  tukey_alpha=p["tukey_alpha"], interp_type=p["interp_type"], channel_scale=w.channel_scale)
+
+    def step():
+        _cuda_impl.beamform_compound(v_ch, storage, v_rx, v_scan, v_arr, v_out, stream=stream.cuda_stream,
+                                     flags=_cuda_impl.FLAG_ASYNC | _cuda_impl.FLAG_OVERWRITE, **common)
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    launches0 = _cuda_impl.launch_count()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    for i in range(args.steps):
+        starts[i].record(stream)
+        step()
+        ends[i].record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    launches = _cuda_impl.launch_count() - launches0
+    clock_info = clocks.stop()
+    per_step = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    total_ms = starts[0].elapsed_time(ends[-1])
+    total_ms = max_over_ranks(total_ms, world)
+    result = out.clone()
+
+    line = {
+        "metric": METRIC,
+        "value": world * w.points * args.steps / (total_ms / 1e3),
+        "unit": "points/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": total_ms / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded simulation of the configuration; no public dataset offline)",
+        "config": {
+            "workload": f"{args.workload}: {WORKLOAD_DESC[args.workload]}",
+            "storage": storage,
+            "n_tx": w.n_tx, "n_rx": w.n_rx, "n_samples": w.n_samples, "n_frames": w.n_frames, "n_vox": w.n_vox,
+            "points_per_step": w.points,
+            "l2": f"inputs larger than L2 ({algorithmic_bytes(w, storage) / 1e6:.0f} MB per step > 126 MB), no flush",
+            "parallelism": f"replicas x{world} (one job per GPU, no exchange)",
+        },
+        "latency_ms": {"p50": float(np.percentile(per_step, 50)), "p99": float(np.percentile(per_step, 99))},
+        "gpu_launches": int(launches),
+    }
+    kernel_s = statistics.mean(per_step) / 1e3
+    peak, peak_kind = measured_peak_hbm()
+    alg = algorithmic_bytes(w, storage)
+    achieved = alg / kernel_s / 1e9
+    line["roofline"] = {
+        "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+        "traffic": profiled_traffic(f"{args.workload}:{storage}"),
+        "algorithmic_bytes_per_launch": alg, "kernel_ms": kernel_s * 1e3, "peak_source": peak_kind,
+    }
+    line["clocks"] = clock_info
+
+    if rank == 0 and world == 1:
+        line.update(accuracy_and_baselines(args, w, storage, result))
+    if not args.no_e2e:
+        line["e2e"] = run_e2e(args, w, storage, ch, world, local)
+    return line
+
+
+def accuracy_and_baselines(args, w, storage, result):
+    """nRMS against the FP64 oracle on a voxel sample (which also gives the CPU baseline rate)."""
+    from oracle import das_fp64, machref, oracle_c
+
+    extra = {}
+    ch_np = storage_numpy(w, storage)
+    src_np = storage_numpy(w, w.storage)
+    keys = ("f_number", "rx_start_s", "sampling_freq_hz", "sound_speed_m_s", "modulation_freq_hz", "tukey_alpha",
+            "interp_type")
+    p = {k: w.params[k] for k in keys}
+    cores = os.cpu_count() or 1
+
+    def oracle_on(n_sub, data, st):
+        sel = np.unique(np.linspace(0, w.n_vox - 1, n_sub).astype(np.int64))
+        t = time.perf_counter()
+        y = oracle_c.beamform_c(data, w.rx_coords_m, w.scan_coords_m, w.tx_wave_arrivals_s, storage=st,
+                                channel_scale=w.channel_scale, voxel_subset=sel, n_threads=cores, **p)
+        return sel, y, time.perf_counter() - t
+
+    n_sub = 256
+    sel, y, dt = oracle_on(n_sub, ch_np, storage)
+    if not args.no_cpu_baseline:
+        while dt < 0.25 * args.cpu_seconds and n_sub < w.n_vox:
+            n_sub = int(min(w.n_vox, n_sub * max(2.0, 0.5 * args.cpu_seconds / max(dt, 1e-3))))
+            sel, y, dt = oracle_on(n_sub, ch_np, storage)
+        pts = len(sel) * w.n_rx * w.n_tx * w.n_frames
+        extra["cpu_baseline"] = {
+            "value": pts / dt, "unit": "points/s", "cores": cores, "kind": "port",
+            "sample": f"{len(sel)} of {w.n_vox} voxels (evenly spaced) x all elements/transmits/frames; "
+                      f"FP64 C restatement (oracle/das_oracle.c), OpenMP, {dt:.1f} s",
+        }
+    got = result.cpu().numpy()[sel]
+    acc = {"nrms_db_vs_fp64_oracle_on_stored_samples": das_fp64.nrms_db(got, y), "oracle_voxels": int(len(sel))}
+    if storage != w.storage:
+        _, y_src, _ = oracle_on(len(sel), src_np, w.storage)
+        acc["nrms_db_vs_fp64_oracle_on_source_data"] = das_fp64.nrms_db(got, y_src)
+    if machref.available() and w.storage in ("c64", "f32", "i16"):
+        ref = reference_once(w)
+        acc["rel_l2_vs_reference_kernel"] = das_fp64.rel_l2(result.cpu().numpy(), ref)
+    extra["accuracy"] = acc
+    return extra
+
+
+def storage_numpy(w, storage):
+    ch = storage_channel(w, storage)
+    if ch.dtype == torch.bfloat16:
+        return ch.view(torch.int16).cpu().numpy().view(np.uint16)
+    return ch.cpu().numpy()
+
+
+def reference_once(w):
+    from oracle import machref
+
+    ch = w.channel
+    if ch.dtype == torch.int16:
+        ch = ch.to(torch.float32) * w.channel_scale
+    ch = ch.cuda().contiguous()
+    rx = torch.as_tensor(w.rx_coords_m, device="cuda")
+    scan = torch.as_tensor(w.scan_coords_m, device="cuda")
+    arr = torch.as_tensor(w.tx_wave_arrivals_s, device="cuda")
+    out = torch.zeros((w.n_vox, w.n_frames), dtype=torch.complex64 if ch.is_complex() else torch.float32,
+                      device="cuda")
+    machref.beamform_device([ch[t].data_ptr() for t in range(w.n_tx)], rx.data_ptr(), scan.data_ptr(),
+                            [arr[t].data_ptr() for t in range(w.n_tx)], out.data_ptr(), is_complex=ch.is_complex(),
+                            n_rx=w.n_rx, n_samples=w.n_samples, n_vox=w.n_vox, n_frames=w.n_frames,
+                            **{k: w.params[k] for k in ("f_number", "rx_start_s", "sampling_freq_hz",
+                                                        "sound_speed_m_s", "modulation_freq_hz", "tukey_alpha",
+                                                        "interp_type")})
+    torch.cuda.synchronize()
+    return out.cpu().numpy()
+
+
+def run_e2e(args, w, storage, ch_dev, world, local):
+    """Same job through the public API with pinned host buffers: H2D + kernel + D2H per step."""
+    from mach_b200 import experimental
+
+    ch_h = ch_dev.cpu().pin_memory()
+    rx_h = torch.as_tensor(w.rx_coords_m).pin_memory()
+    scan_h = torch.as_tensor(w.scan_coords_m).pin_memory()
+    arr_h = torch.as_tensor(w.tx_wave_arrivals_s).pin_memory()
+    is_c = storage in ("c64", "cf16", "cbf16", "ci16")
+    out_h = torch.zeros((w.n_vox, w.n_frames), dtype=torch.complex64 if is_c else torch.float32).pin_memory()
+
+    def step():
+        with warnings.catch_warnings():
+            warnings.simplefilter("ignore", UserWarning)
+            experimental.beamform(ch_h, rx_h, scan_h, arr_h, out=out_h, channel_scale=w.channel_scale, **w.params)
+
+    for _ in range(max(1, min(args.warmup, 3))):
+        step()
+    torch.cuda.synchronize()
+    barrier(world)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+    torch.cuda.synchronize()
+    dt = max_over_ranks(time.perf_counter() - t0, world)
+    h2d = ch_h.numel() * ch_h.element_size() + rx_h.numel() * 4 + scan_h.numel() * 4 + arr_h.numel() * 4
+    d2h = out_h.numel() * out_h.element_size()
+    return {"value": world * w.points * args.steps / dt, "unit": "points/s", "h2d_bytes_per_step": int(h2d),
+            "d2h_bytes_per_step": int(d2h), "ms_per_step": dt / args.steps * 1e3,
+            "api": "mach_b200.experimental.beamform with pinned host tensors"}
+
+
+# ----------------------------------------------------------------------------- reference arm
+
+
+def run_reference(args, world, rank, local):
+    from oracle import machref
+
+    base = {"metric": METRIC, "unit": "points/s", "impl": "reference", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": True}
+    if not machref.available():
+        return {"impl": "reference", "unavailable": "mach's kernel was not built into oracle/_ref (no reference checkout)"}
+    w = make_workload(args.workload)
+    ch = w.channel
+    if ch.dtype == torch.int16:
+        ch = ch.to(torch.float32) * w.channel_scale
+    ch = ch.contiguous()
+    is_c = ch.is_complex()
+    rx = torch.as_tensor(w.rx_coords_m, device="cuda")
+    scan = torch.as_tensor(w.scan_coords_m, device="cuda")
+    arr = torch.as_tensor(w.tx_wave_arrivals_s, device="cuda")
+    out = torch.zeros((w.n_vox, w.n_frames), dtype=torch.complex64 if is_c else torch.float32, device="cuda")
+    keys = ("f_number", "rx_start_s", "sampling_freq_hz", "sound_speed_m_s", "modulation_freq_hz", "tukey_alpha",
+            "interp_type")
+    p = {k: w.params[k] for k in keys}
+    ch_ptrs = [ch[t].data_ptr() for t in range(w.n_tx)]
+    arr_ptrs = [arr[t].data_ptr() for t in range(w.n_tx)]
+
+    def step():
+        out.zero_()
+        machref.beamform_device(ch_ptrs, rx.data_ptr(), scan.data_ptr(), arr_ptrs, out.data_ptr(), is_complex=is_c,
+                                n_rx=w.n_rx, n_samples=w.n_samples, n_vox=w.n_vox, n_frames=w.n_frames, **p)
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    lat = []
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        s = time.perf_counter()
+        step()
+        torch.cuda.synchronize()
+        lat.append((time.perf_counter() - s) * 1e3)
+    dt = time.perf_counter() - t0
+    clock_info = clocks.stop()
+    line = dict(base)
+    line.update({
+        "value": w.points * args.steps / dt,
+        "ms_per_step": dt / args.steps * 1e3,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded simulation of the configuration; no public dataset offline)",
+        "config": {"workload": f"{args.workload}: {WORKLOAD_DESC[args.workload]}",
+                   "storage": "c64" if is_c else "f32", "n_tx": w.n_tx, "n_rx": w.n_rx, "n_samples": w.n_samples,
+                   "n_frames": w.n_frames, "n_vox": w.n_vox, "points_per_step": w.points,
+                   "l2": "inputs larger than L2, no flush",
+                   "parallelism": "rank 0 only"},
+        "reference": "mach 0.1.3 src/mach/kernel.cu compiled for sm_100a from its unmodified source; one launch + "
+                     "cudaDeviceSynchronize per transmit into a zeroed complex64/float32 out (mach.experimental loop)",
+        "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
+        "clocks": clock_info,
+        "gpu_launches": w.n_tx * args.steps,
+    })
+    if not args.no_e2e:
+        ch_h = ch.cpu().pin_memory()
+        rx_h, scan_h = w.rx_coords_m, w.scan_coords_m
+        arr_h = np.ascontiguousarray(w.tx_wave_arrivals_s)
+        ch_np = ch_h.numpy()
+        out_h = torch.zeros_like(out, device="cpu").pin_memory()
+
+        def e2e_step():
+            out.zero_()
+            machref.beamform_host(ch_np, rx_h, scan_h, arr_h, None, out_on_device_ptr=out.data_ptr(), **p)
+            out_h.copy_(out)
+
+        e2e_step()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            e2e_step()
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        per_tx = ch_np[0].nbytes + arr_h[0].nbytes + rx_h.nbytes + scan_h.nbytes
+        line["e2e"] = {"value": w.points * args.steps / dt, "unit": "points/s",
+                       "h2d_bytes_per_step": int(per_tx * w.n_tx), "d2h_bytes_per_step": int(out_h.numel() * 8 if is_c else out_h.numel() * 4),
+                       "ms_per_step": dt / args.steps * 1e3,
+                       "api": "mach's binding with host arrays per transmit (its CPU staging path), device out"}
+    return line
+
+
+def main():
+    args = parse_args()
+    world, rank, local = dist_setup()
+    try:
+        if args.impl == "reference":
+            if rank != 0:
+                return
+            line = run_reference(args, world, rank, local)
+        else:
+            line = run_ours(args, world, rank, local)
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+    finally:
+        if world > 1 and torch.distributed.is_initialized():
+            torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

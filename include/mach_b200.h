@@ -1,0 +1,123 @@
+/*
+ * mach_b200 -- C ABI of the B200 delay-and-sum beamformer.
+ *
+ * Plain pointers, sizes and scalars only.  Every pointer may be device memory
+ * (cudaMalloc / managed) or host memory (pinned or pageable); host buffers are
+ * staged through the GPU the way mach's binding stages CPU arrays
+ * (src/mach/kernel.cu:1090-1208): host inputs are copied in, and a host `out`
+ * is OVERWRITTEN with the result, while a device `out` is ACCUMULATED into
+ * (src/mach/kernel.cu:675-680, 1135-1139, 1203-1205).
+ *
+ * Every function returns MACH_B200_OK (0) or an error code; the message of the
+ * last failure on the calling thread is available from mach_b200_last_error().
+ * No function terminates the process (mach's helper_cuda.h exits on CUDA errors).
+ *
+ * Layouts (C order):
+ *   channel_data        [n_tx][n_rx][n_samples][n_frames] samples of `storage`
+ *   rx_coords_m         [n_rx][3]   float32, metres
+ *   scan_coords_m       [n_scan][3] float32, metres
+ *   tx_wave_arrivals_s  [n_tx][n_scan] float32, seconds
+ *   out                 [n_scan][n_frames] float32 (real storage) or complex64 (complex storage)
+ */
+#ifndef MACH_B200_H_
+#define MACH_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define MACH_B200_API __attribute__((visibility("default")))
+#else
+#define MACH_B200_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. */
+#define MACH_B200_OK 0
+#define MACH_B200_ERR_VALUE 1 /* bad argument: shape, range, dtype (mach raises RuntimeError) */
+#define MACH_B200_ERR_CUDA 2  /* a CUDA runtime call failed */
+#define MACH_B200_ERR_DEVICE 3 /* pointer on another device than the current one */
+
+/* Interpolation (mach InterpolationType, src/mach/kernel.cu:25-29). */
+#define MACH_B200_NEAREST 0
+#define MACH_B200_LINEAR 1
+#define MACH_B200_QUADRATIC 2
+
+/* Channel-data storage.  Odd codes are complex (I, Q) pairs.  All arithmetic is FP32. */
+#define MACH_B200_STORAGE_F32 0   /* float32 RF (mach's float overload) */
+#define MACH_B200_STORAGE_C64 1   /* complex64 IQ (mach's complex64 overload) */
+#define MACH_B200_STORAGE_F16 2   /* binary16 RF */
+#define MACH_B200_STORAGE_CF16 3  /* binary16 IQ pairs */
+#define MACH_B200_STORAGE_BF16 4  /* bfloat16 RF */
+#define MACH_B200_STORAGE_CBF16 5 /* bfloat16 IQ pairs */
+#define MACH_B200_STORAGE_I16 6   /* int16 RF, value = sample * channel_scale */
+#define MACH_B200_STORAGE_CI16 7  /* int16 IQ pairs, value = sample * channel_scale */
+
+/* Flags for mach_b200_beamform_compound. */
+#define MACH_B200_FLAG_ASYNC 1u     /* return without synchronising `cuda_stream` (device buffers only) */
+#define MACH_B200_FLAG_OVERWRITE 2u /* out = result instead of out += result */
+
+/*
+ * Single-transmit DAS on float32 RF, synchronous on the legacy default stream.
+ * Replaces the float32 overload of mach._cuda_impl.beamform
+ * (src/mach/kernel.cu:1242-1255, body 1032-1209; stub src/mach/_cuda_impl.pyi:39-53).
+ */
+MACH_B200_API int mach_b200_beamform_f32(const float* channel_data, const float* rx_coords_m,
+                           const float* scan_coords_m, const float* tx_wave_arrivals_s,
+                           float* out, uint32_t n_rx, uint32_t n_samples, uint64_t n_scan,
+                           uint32_t n_frames, float f_number, float rx_start_s,
+                           float sampling_freq_hz, float sound_speed_m_s,
+                           float modulation_freq_hz, float tukey_alpha, int32_t interp_type);
+
+/*
+ * Single-transmit DAS on complex64 IQ (interleaved float pairs), synchronous on the
+ * legacy default stream.  Replaces the complex64 overload of mach._cuda_impl.beamform
+ * (src/mach/kernel.cu:1229-1241, body 1032-1209; stub src/mach/_cuda_impl.pyi:24-38).
+ */
+MACH_B200_API int mach_b200_beamform_c64(const void* channel_data, const float* rx_coords_m,
+                           const float* scan_coords_m, const float* tx_wave_arrivals_s,
+                           void* out, uint32_t n_rx, uint32_t n_samples, uint64_t n_scan,
+                           uint32_t n_frames, float f_number, float rx_start_s,
+                           float sampling_freq_hz, float sound_speed_m_s,
+                           float modulation_freq_hz, float tukey_alpha, int32_t interp_type);
+
+/*
+ * Coherent compounding over n_tx transmits in ONE launch, any storage type, on
+ * `cuda_stream` (a cudaStream_t; NULL = legacy default stream).  Replaces the
+ * per-transmit loop of mach.experimental.beamform (src/mach/experimental.py:23-108,
+ * loop 80-97), which launches and synchronises once per transmit.  With host
+ * inputs the transmits are copied in chunks on a second stream while earlier
+ * chunks compute.  Synchronous unless MACH_B200_FLAG_ASYNC is set and every
+ * buffer is device memory.
+ */
+MACH_B200_API int mach_b200_beamform_compound(int32_t storage, const void* channel_data,
+                                const float* rx_coords_m, const float* scan_coords_m,
+                                const float* tx_wave_arrivals_s, void* out, uint32_t n_tx,
+                                uint32_t n_rx, uint32_t n_samples, uint64_t n_scan,
+                                uint32_t n_frames, float f_number, float rx_start_s,
+                                float sampling_freq_hz, float sound_speed_m_s,
+                                float modulation_freq_hz, float tukey_alpha,
+                                int32_t interp_type, float channel_scale, void* cuda_stream,
+                                uint32_t flags);
+
+/* Message of the last failed call on this thread ("" if none). */
+MACH_B200_API const char* mach_b200_last_error(void);
+
+/* nvcc version the library was built with, "X.Y.Z" (mach's __nvcc_version__,
+ * src/mach/kernel.cu:1215). */
+MACH_B200_API const char* mach_b200_nvcc_version(void);
+
+/* Library version string. */
+MACH_B200_API const char* mach_b200_version(void);
+
+/* Number of kernels this library has launched since it was loaded. */
+MACH_B200_API uint64_t mach_b200_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MACH_B200_H_ */

@@ -1,0 +1,136 @@
+"""Coherent compounding over transmits (mirror of mach's src/mach/experimental.py:23-108).
+
+mach loops over transmits in Python and launches (and synchronises) its kernel once
+per transmit, always with linear interpolation.  Here all transmits go to the GPU in
+one launch of ``mach_b200_beamform_compound``: each (voxel, element) receive path is
+computed once and reused for every transmit, the sum stays in registers and ``out``
+is written once.  ``interp_type`` is honoured, and channel data may be stored as
+float32 / complex64 or, for reduced-precision storage, float16, bfloat16 or int16
+(real, or complex as a trailing (I, Q) axis; torch ``complex32`` is also accepted).
+All arithmetic is FP32.
+"""
+
+from __future__ import annotations
+
+import warnings
+from typing import Any
+
+from mach_b200 import _cuda_impl, _dlpack
+from mach_b200._array_api import array_namespace, is_writeable_array
+from mach_b200._check import ensure_contiguous, is_contiguous
+from mach_b200._cuda_impl import InterpolationType
+
+
+def _current_stream(x: Any) -> int:
+    if _dlpack.is_torch(x) and x.device.type == "cuda":
+        import torch
+
+        return int(torch.cuda.current_stream(x.device).cuda_stream)
+    return 0
+
+
+def beamform(
+    channel_data: Any,
+    rx_coords_m: Any,
+    scan_coords_m: Any,
+    tx_wave_arrivals_s: Any,
+    out: Any = None,
+    *,
+    rx_start_s: float,
+    sampling_freq_hz: float,
+    f_number: float,
+    sound_speed_m_s: float,
+    modulation_freq_hz: float | None = None,
+    tukey_alpha: float = 0.5,
+    interp_type: InterpolationType = InterpolationType.Linear,
+    channel_scale: float = 1.0,
+    sync: bool = True,
+) -> Any:
+    """Beamform and coherently compound ``n_transmits`` transmits.
+
+    Args:
+        channel_data: ``[n_transmits, n_rx, n_samples, n_frames]`` (float32, float64,
+            complex64, complex128, float16, bfloat16, int16, torch complex32) or
+            ``[n_transmits, n_rx, n_samples, n_frames, 2]`` (I, Q) pairs of float16 /
+            bfloat16 / int16.
+        tx_wave_arrivals_s: ``[n_transmits, n_points]`` seconds.
+        channel_scale: multiplier applied to every sample (for int16 storage).
+        sync: when False and every array is on the GPU, return without waiting for the
+            kernel (it runs on the current torch stream for torch inputs).
+        Other arguments as in :func:`mach_b200.kernel.beamform`.
+
+    Returns:
+        ``out[n_points, n_frames]``: complex64 for complex storage, float32 otherwise.
+        A GPU ``out`` is accumulated into; a CPU ``out`` is overwritten (as in mach).
+    """
+    xp = array_namespace(channel_data)
+    complex_pairs = len(channel_data.shape) == 5
+    if complex_pairs and channel_data.shape[-1] != 2:
+        raise ValueError("a 5-D channel_data must end in an (I, Q) axis of length 2")
+    if not complex_pairs and len(channel_data.shape) != 4:
+        raise ValueError("channel_data must be [n_transmits, n_rx, n_samples, n_frames]")
+    dtype_name = str(channel_data.dtype).replace("torch.", "")
+    if dtype_name == "complex128":
+        channel_data = xp.astype(channel_data, xp.complex64, copy=False)
+    elif dtype_name == "float64":
+        channel_data = xp.astype(channel_data, xp.float32, copy=False)
+    channel_data = ensure_contiguous(channel_data)
+    ch = _dlpack.view(channel_data)
+    storage = _cuda_impl.storage_of(ch, complex_pairs)
+    is_complex = bool(_cuda_impl.STORAGE_CODES[storage] & 1)
+    if is_complex and modulation_freq_hz is None:
+        raise ValueError(
+            "modulation_freq_hz is required for complex phase-correction. set it to 0 if no demodulation was used."
+        )
+    if modulation_freq_hz is None:
+        modulation_freq_hz = 0.0
+
+    xpc = array_namespace(rx_coords_m)
+    xps = array_namespace(scan_coords_m)
+    xpa = array_namespace(tx_wave_arrivals_s)
+    rx_coords_m = ensure_contiguous(xpc.astype(rx_coords_m, xpc.float32, copy=False))
+    scan_coords_m = ensure_contiguous(xps.astype(scan_coords_m, xps.float32, copy=False))
+    tx_wave_arrivals_s = ensure_contiguous(xpa.astype(tx_wave_arrivals_s, xpa.float32, copy=False))
+
+    n_tx, n_rx, n_samples, n_frames = (int(d) for d in channel_data.shape[:4])
+    n_points = int(scan_coords_m.shape[0])
+    output_dtype = xp.complex64 if is_complex else xp.float32
+    if out is None:
+        out = xp.zeros((n_points, n_frames), dtype=output_dtype, like=channel_data)
+    elif out.dtype != output_dtype:
+        raise ValueError(f"Output array dtype {out.dtype} doesn't match expected {output_dtype}")
+    if not is_writeable_array(out):
+        raise ValueError("Output array `out` is not writable. Try using cupy or pytorch for the output array.")
+    if not is_contiguous(out):
+        raise ValueError("Output array `out` must be contiguous.")
+
+    rx = _dlpack.view(rx_coords_m)
+    scan = _dlpack.view(scan_coords_m)
+    arr = _dlpack.view(tx_wave_arrivals_s)
+    o = _dlpack.view(out)
+    if tuple(rx.shape) != (n_rx, 3):
+        raise RuntimeError(f"rx_coords_m.shape {list(rx.shape)} must be [{n_rx}, 3]")
+    if tuple(scan.shape) != (n_points, 3):
+        raise RuntimeError(f"scan_coords_m.shape {list(scan.shape)} must be [n_points, 3]")
+    if tuple(arr.shape) != (n_tx, n_points):
+        raise RuntimeError(f"tx_wave_arrivals_s.shape {list(arr.shape)} must be [{n_tx}, {n_points}]")
+    if tuple(o.shape) != (n_points, n_frames):
+        raise RuntimeError(f"out.shape {list(o.shape)} must be [{n_points}, {n_frames}]")
+    cpu = sum(v.device_type == _dlpack.CPU for v in (ch, rx, scan, arr))
+    if cpu:
+        warnings.warn(
+            f"Found {cpu} input array(s) on CPU. This will add latency due to CPU<->GPU memory transfers. "
+            "For optimal performance with CUDA beamforming, move arrays to GPU using cupy, jax, or similar.",
+            UserWarning,
+            stacklevel=2,
+        )
+    all_gpu = all(v.on_cuda for v in (ch, rx, scan, arr, o))
+    flags = 0 if (sync or not all_gpu) else _cuda_impl.FLAG_ASYNC
+    _cuda_impl.beamform_compound(
+        ch, storage, rx, scan, arr, o, n_tx=n_tx, n_rx=n_rx, n_samples=n_samples, n_vox=n_points,
+        n_frames=n_frames, f_number=f_number, rx_start_s=rx_start_s, sampling_freq_hz=sampling_freq_hz,
+        sound_speed_m_s=sound_speed_m_s, modulation_freq_hz=modulation_freq_hz, tukey_alpha=tukey_alpha,
+        interp_type=int(interp_type), channel_scale=channel_scale, stream=_current_stream(channel_data),
+        flags=flags,
+    )
+    return out
