@@ -168,10 +168,14 @@ def make_workload(name: str):
     from mach_b200 import workloads as W
 
     if name == "volume3d":
-        return W.volume3d(n_frames=1, device="cuda")
-    if name == "volume3d16":
-        return W.volume3d(n_frames=16, device="cuda")
-    return W.CONFIGS[name](device="cuda")
+        w = W.volume3d(n_frames=1, device="cuda")
+    elif name == "volume3d16":
+        w = W.volume3d(n_frames=16, device="cuda")
+    else:
+        w = W.CONFIGS[name](device="cuda")
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()  # drop the synthesis temporaries
+    return w
 
 
 def storage_channel(w, storage):

@@ -42,7 +42,7 @@ def _load():
             ctypes.c_size_t,
         ]
         lib.machref_beamform_impl.restype = ctypes.c_int
-        lib.machref_beamform_impl.argtypes = [ctypes.c_int] + [ctypes.c_void_p] * 6 + common
+        lib.machref_beamform_impl.argtypes = [ctypes.c_int] + [ctypes.c_void_p] * 5 + common
         lib.machref_beamform_binding.restype = ctypes.c_int
         lib.machref_beamform_binding.argtypes = [
             ctypes.c_int,
