@@ -59,6 +59,7 @@ def parse_args():
     p.add_argument("--cpu-seconds", type=float, default=10.0, help="target CPU time of the cpu_baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--frames", type=int, default=None, help="override the workload's frame count (profiling)")
     return p.parse_args()
 
 
@@ -164,13 +165,15 @@ def profiled_traffic(key: str):
 # ----------------------------------------------------------------------------- workloads
 
 
-def make_workload(name: str):
+def make_workload(name: str, frames: int | None = None):
     from mach_b200 import workloads as W
 
     if name == "volume3d":
-        w = W.volume3d(n_frames=1, device="cuda")
+        w = W.volume3d(n_frames=frames or 1, device="cuda")
     elif name == "volume3d16":
-        w = W.volume3d(n_frames=16, device="cuda")
+        w = W.volume3d(n_frames=frames or 16, device="cuda")
+    elif name == "doppler" and frames:
+        w = W.doppler(n_frames=frames, device="cuda")
     else:
         w = W.CONFIGS[name](device="cuda")
     torch.cuda.synchronize()
@@ -197,7 +200,7 @@ def algorithmic_bytes(w, storage) -> int:
 def run_ours(args, world, rank, local):
     from mach_b200 import _cuda_impl, _dlpack, experimental
 
-    w = make_workload(args.workload)
+    w = make_workload(args.workload, args.frames)
     storage = args.storage or w.storage
     ch = storage_channel(w, storage)
     dev = torch.device("cuda", local)
@@ -214,9 +217,14 @@ def run_ours(args, world, rank, local):
                   sound_speed_m_s=p["sound_speed_m_s"], modulation_freq_hz=p["modulation_freq_hz"],
                   tukey_alpha=p["tukey_alpha"], interp_type=p["interp_type"], channel_scale=w.channel_scale)
 
+    from mach_b200 import _grid
+
+    options = _cuda_impl.make_options(grid_shape=_grid.detect(w.scan_coords_m))
+
     def step():
         _cuda_impl.beamform_compound(v_ch, storage, v_rx, v_scan, v_arr, v_out, stream=stream.cuda_stream,
-                                     flags=_cuda_impl.FLAG_ASYNC | _cuda_impl.FLAG_OVERWRITE, **common)
+                                     flags=_cuda_impl.FLAG_ASYNC | _cuda_impl.FLAG_OVERWRITE, options=options,
+                                     **common)
 
     clocks = ClockSampler(local)
     clocks.start()
@@ -277,10 +285,10 @@ def run_ours(args, world, rank, local):
     }
     line["clocks"] = clock_info
 
-    if rank == 0 and world == 1:
-        line.update(accuracy_and_baselines(args, w, storage, result))
     if not args.no_e2e:
         line["e2e"] = run_e2e(args, w, storage, ch, world, local)
+    if rank == 0 and world == 1:
+        line.update(accuracy_and_baselines(args, w, storage, result))
     return line
 
 
@@ -398,7 +406,7 @@ def run_reference(args, world, rank, local):
             "warmup": args.warmup, "higher_is_better": True}
     if not machref.available():
         return {"impl": "reference", "unavailable": "mach's kernel was not built into oracle/_ref (no reference checkout)"}
-    w = make_workload(args.workload)
+    w = make_workload(args.workload, args.frames)
     ch = w.channel
     if ch.dtype == torch.int16:
         ch = ch.to(torch.float32) * w.channel_scale

@@ -56,9 +56,32 @@ extern "C" {
 #define MACH_B200_STORAGE_I16 6   /* int16 RF, value = sample * channel_scale */
 #define MACH_B200_STORAGE_CI16 7  /* int16 IQ pairs, value = sample * channel_scale */
 
-/* Flags for mach_b200_beamform_compound. */
+/* Flags for mach_b200_beamform_compound / mach_b200_beamform_ex. */
 #define MACH_B200_FLAG_ASYNC 1u     /* return without synchronising `cuda_stream` (device buffers only) */
 #define MACH_B200_FLAG_OVERWRITE 2u /* out = result instead of out += result */
+
+/* Kernel families (mach_b200_options.kernel). */
+#define MACH_B200_KERNEL_AUTO 0
+#define MACH_B200_KERNEL_LANE_VOXEL 1 /* one lane per voxel, all frames in registers (1..8 frames) */
+#define MACH_B200_KERNEL_STAGED 2     /* voxel tiles, sample windows staged in shared memory by TMA */
+#define MACH_B200_KERNEL_WARP 3       /* a warp per voxel over frames, taps read from global memory */
+
+/*
+ * Optional launch options.  Zero-initialise, set struct_size = sizeof(mach_b200_options),
+ * then set what you need.  Every field only affects speed, never the result.
+ */
+typedef struct mach_b200_options {
+    uint32_t struct_size;   /* sizeof(mach_b200_options) */
+    uint32_t flags;         /* MACH_B200_FLAG_* */
+    int32_t grid_shape[3];  /* scan_coords_m as a C-order grid (slow, mid, fast), fast = contiguous
+                               axis (e.g. (nx, 1, nz) for a meshgrid(x, [y0], z, indexing="ij")
+                               flattened); zeros = no grid: tiles are runs of consecutive voxels */
+    int32_t kernel;          /* MACH_B200_KERNEL_*, 0 = automatic */
+    int32_t tx_chunk;        /* lane-voxel kernel: transmits per shared-memory pass, 0 = automatic */
+    int32_t window_rows;     /* staged kernel: sample rows per staged window, 0 = automatic */
+    int32_t lanes_per_voxel; /* staged kernel: 4, 8, 16 or 32, 0 = automatic */
+    int32_t reserved[4];
+} mach_b200_options;
 
 /*
  * Single-transmit DAS on float32 RF, synchronous on the legacy default stream.
@@ -102,6 +125,20 @@ MACH_B200_API int mach_b200_beamform_compound(int32_t storage, const void* chann
                                 float modulation_freq_hz, float tukey_alpha,
                                 int32_t interp_type, float channel_scale, void* cuda_stream,
                                 uint32_t flags);
+
+/*
+ * mach_b200_beamform_compound with launch options (grid hint and tuning knobs chosen by
+ * the autotuner).  `options` may be NULL.  Same semantics and errors as the compound call.
+ */
+MACH_B200_API int mach_b200_beamform_ex(int32_t storage, const void* channel_data,
+                                const float* rx_coords_m, const float* scan_coords_m,
+                                const float* tx_wave_arrivals_s, void* out, uint32_t n_tx,
+                                uint32_t n_rx, uint32_t n_samples, uint64_t n_scan,
+                                uint32_t n_frames, float f_number, float rx_start_s,
+                                float sampling_freq_hz, float sound_speed_m_s,
+                                float modulation_freq_hz, float tukey_alpha,
+                                int32_t interp_type, float channel_scale, void* cuda_stream,
+                                const mach_b200_options* options);
 
 /* Message of the last failed call on this thread ("" if none). */
 MACH_B200_API const char* mach_b200_last_error(void);

@@ -41,6 +41,46 @@ _lib.mach_b200_beamform_compound.argtypes = [
     _I32, _P, _P, _P, _P, _P, _U32, _U32, _U32, _U64, _U32, _F, _F, _F, _F, _F, _F, _I32, _F, _P, _U32,
 ]
 _lib.mach_b200_beamform_compound.restype = ctypes.c_int
+
+
+class Options(ctypes.Structure):
+    """``mach_b200_options`` (include/mach_b200.h): launch hints that never change the result."""
+
+    _fields_ = [
+        ("struct_size", ctypes.c_uint32),
+        ("flags", ctypes.c_uint32),
+        ("grid_shape", ctypes.c_int32 * 3),
+        ("kernel", ctypes.c_int32),
+        ("tx_chunk", ctypes.c_int32),
+        ("window_rows", ctypes.c_int32),
+        ("lanes_per_voxel", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 4),
+    ]
+
+
+KERNELS = {"auto": 0, "lane_voxel": 1, "staged": 2, "warp": 3}
+
+
+def make_options(flags: int = 0, grid_shape=None, kernel: str | int = 0, tx_chunk: int = 0, window_rows: int = 0,
+                 lanes_per_voxel: int = 0) -> Options:
+    o = Options()
+    o.struct_size = ctypes.sizeof(Options)
+    o.flags = int(flags)
+    if grid_shape is not None:
+        for i, v in enumerate(grid_shape):
+            o.grid_shape[i] = int(v)
+    o.kernel = KERNELS[kernel] if isinstance(kernel, str) else int(kernel)
+    o.tx_chunk = int(tx_chunk)
+    o.window_rows = int(window_rows)
+    o.lanes_per_voxel = int(lanes_per_voxel)
+    return o
+
+
+_lib.mach_b200_beamform_ex.argtypes = [
+    _I32, _P, _P, _P, _P, _P, _U32, _U32, _U32, _U64, _U32, _F, _F, _F, _F, _F, _F, _I32, _F, _P,
+    ctypes.POINTER(Options),
+]
+_lib.mach_b200_beamform_ex.restype = ctypes.c_int
 _lib.mach_b200_last_error.restype = ctypes.c_char_p
 _lib.mach_b200_nvcc_version.restype = ctypes.c_char_p
 _lib.mach_b200_version.restype = ctypes.c_char_p
@@ -246,12 +286,17 @@ def beamform_compound(
     channel_scale: float = 1.0,
     stream: int = 0,
     flags: int = 0,
+    options: Options | None = None,
 ) -> None:
-    """Multi-transmit DAS in one launch through ``mach_b200_beamform_compound``."""
-    rc = _lib.mach_b200_beamform_compound(
+    """Multi-transmit DAS in one launch through ``mach_b200_beamform_ex``."""
+    if options is None:
+        options = make_options(flags)
+    else:
+        options.flags = int(flags)
+    rc = _lib.mach_b200_beamform_ex(
         STORAGE_CODES[storage], channel.ptr, rx.ptr, scan.ptr, arrivals.ptr, out.ptr, n_tx, n_rx, n_samples,
         n_vox, n_frames, float(f_number), float(rx_start_s), float(sampling_freq_hz), float(sound_speed_m_s),
         float(modulation_freq_hz), float(tukey_alpha), int(interp_type), float(channel_scale), stream or None,
-        int(flags),
+        ctypes.byref(options),
     )
     _raise_for(rc)

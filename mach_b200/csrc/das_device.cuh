@@ -124,7 +124,8 @@ struct DasArgs {
     int32_t apod;           // tukey_alpha > 0 (kernel.cu:749)
     int32_t rotate;         // complex storage and f_mod != 0 (kernel.cu:653)
     int32_t accumulate;     // out += result (reference semantics) instead of out = result
-    int32_t frame_passes;   // frames handled per lane
+    int32_t frame_passes;   // frames handled per lane (multi-frame kernel)
+    int32_t tx_chunk;       // transmits whose arrivals are staged in shared memory at once
 };
 
 // Half-Tukey weight of r = horizontal distance / aperture radius (kernel.cu:333-349).

@@ -213,47 +213,4 @@ __global__ void __launch_bounds__(kThreadsPerBlock) das_gather_kernel(const __gr
     }
 }
 
-// Lane shapes instantiated for every storage / interpolation pair.
-enum ShapeCode : int {
-    kShapeOneFrame = 0,   // LPV 1, 1 frame per lane       (n_frames == 1)
-    kShapeFewFrames = 1,  // LPV 1, up to 8 frames per lane (2 <= n_frames <= 8)
-    kShapeHalfWarp = 2,   // LPV 16, up to 4 frames per lane
-    kShapeWarp = 3,       // LPV 32, up to 8 frames per lane
-};
-
-struct ShapeInfo {
-    int lpv;
-    int max_passes;
-};
-
-inline ShapeInfo shape_info(int shape) {
-    switch (shape) {
-        case kShapeOneFrame: return {1, 1};
-        case kShapeFewFrames: return {1, 8};
-        case kShapeHalfWarp: return {16, 4};
-        default: return {32, 8};
-    }
-}
-
-// Launch one kernel instance.  Returns the launch error (cudaSuccess when queued).
-template <int S>
-cudaError_t launch_das_gather(const DasArgs& a, int interp, int shape, dim3 grid, cudaStream_t stream) {
-#define MACH_B200_LAUNCH(I, L, P) das_gather_kernel<S, I, L, P><<<grid, kThreadsPerBlock, 0, stream>>>(a)
-#define MACH_B200_SHAPES(I)                          \
-    switch (shape) {                                 \
-        case kShapeOneFrame: MACH_B200_LAUNCH(I, 1, 1); break;   \
-        case kShapeFewFrames: MACH_B200_LAUNCH(I, 1, 8); break;  \
-        case kShapeHalfWarp: MACH_B200_LAUNCH(I, 16, 4); break;  \
-        default: MACH_B200_LAUNCH(I, 32, 8); break;              \
-    }
-    switch (interp) {
-        case kNearest: MACH_B200_SHAPES(kNearest); break;
-        case kLinear: MACH_B200_SHAPES(kLinear); break;
-        default: MACH_B200_SHAPES(kQuadratic); break;
-    }
-#undef MACH_B200_SHAPES
-#undef MACH_B200_LAUNCH
-    return cudaGetLastError();
-}
-
 }  // namespace mach_b200

@@ -1,7 +1,9 @@
 // Gather kernels for f32 channel-data storage (one translation unit per storage type
 // so the library compiles in parallel).
-#include "das_gather.cuh"
+#include "das_launch.cuh"
 
 namespace mach_b200 {
-template cudaError_t launch_das_gather<kF32>(const DasArgs&, int, int, dim3, cudaStream_t);
+template cudaError_t launch_das<kF32>(const DasArgs&, int, const LaunchPlan&, cudaStream_t);
+template cudaError_t launch_das_staged<kF32>(const DasArgs&, const StagedArgs&, const CUtensorMap&, int,
+                                             const LaunchPlan&, cudaStream_t);
 }  // namespace mach_b200

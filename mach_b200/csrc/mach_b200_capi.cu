@@ -1,30 +1,43 @@
 // C ABI of mach_b200 (declared in include/mach_b200.h): argument checks, host-buffer
-// staging, launch planning and the kernel dispatch.
+// staging, launch planning (kernel family, tiling, TMA descriptor) and dispatch.
+#include <cudaTypedefs.h>
+
 #include <algorithm>
 #include <atomic>
 #include <cstdarg>
+#include <cstddef>
 #include <cstdio>
+#include <cstring>
+#include <mutex>
 #include <string>
 
-#include "das_gather.cuh"
+#include "das_launch.cuh"
 #include "mach_b200.h"
 
 #ifndef MACH_B200_NVCC_VERSION
 #define MACH_B200_NVCC_VERSION "0.0.0"
 #endif
-#define MACH_B200_VERSION "0.1.0"
+#define MACH_B200_VERSION "0.2.0"
 
 namespace mach_b200 {
 // Instantiated once per storage type in das_gather_<storage>.cu.
-extern template cudaError_t launch_das_gather<kF32>(const DasArgs&, int, int, dim3, cudaStream_t);
-extern template cudaError_t launch_das_gather<kC64>(const DasArgs&, int, int, dim3, cudaStream_t);
-extern template cudaError_t launch_das_gather<kF16>(const DasArgs&, int, int, dim3, cudaStream_t);
-extern template cudaError_t launch_das_gather<kCF16>(const DasArgs&, int, int, dim3, cudaStream_t);
-extern template cudaError_t launch_das_gather<kBF16>(const DasArgs&, int, int, dim3, cudaStream_t);
-extern template cudaError_t launch_das_gather<kCBF16>(const DasArgs&, int, int, dim3, cudaStream_t);
-extern template cudaError_t launch_das_gather<kI16>(const DasArgs&, int, int, dim3, cudaStream_t);
-extern template cudaError_t launch_das_gather<kCI16>(const DasArgs&, int, int, dim3, cudaStream_t);
+#define MACH_B200_EXTERN(S)                                                                                  \
+    extern template cudaError_t launch_das<S>(const DasArgs&, int, const LaunchPlan&, cudaStream_t);         \
+    extern template cudaError_t launch_das_staged<S>(const DasArgs&, const StagedArgs&, const CUtensorMap&, \
+                                                     int, const LaunchPlan&, cudaStream_t);
+MACH_B200_EXTERN(kF32)
+MACH_B200_EXTERN(kC64)
+MACH_B200_EXTERN(kF16)
+MACH_B200_EXTERN(kCF16)
+MACH_B200_EXTERN(kBF16)
+MACH_B200_EXTERN(kCBF16)
+MACH_B200_EXTERN(kI16)
+MACH_B200_EXTERN(kCI16)
+#undef MACH_B200_EXTERN
 }  // namespace mach_b200
+
+// Status word written by kernels whose bounded waits time out (one per device).
+__device__ int g_mach_b200_status;
 
 namespace {
 
@@ -43,12 +56,12 @@ int fail(int code, const char* fmt, ...) {
     return code;
 }
 
-#define MACH_B200_CUDA_TRY(expr)                                                                  \
-    do {                                                                                          \
-        cudaError_t err_ = (expr);                                                                \
-        if (err_ != cudaSuccess) {                                                                \
-            return fail(MACH_B200_ERR_CUDA, "%s failed: %s", #expr, cudaGetErrorString(err_));   \
-        }                                                                                         \
+#define MACH_B200_CUDA_TRY(expr)                                                                \
+    do {                                                                                        \
+        cudaError_t err_ = (expr);                                                              \
+        if (err_ != cudaSuccess) {                                                              \
+            return fail(MACH_B200_ERR_CUDA, "%s failed: %s", #expr, cudaGetErrorString(err_)); \
+        }                                                                                       \
     } while (0)
 
 size_t storage_bytes(int storage) {
@@ -75,9 +88,8 @@ int residency(const void* p, int device, Residency* r, const char* name) {
         case cudaMemoryTypeDevice:
         case cudaMemoryTypeManaged:
             if (attr.type == cudaMemoryTypeDevice && attr.device != device) {
-                return fail(MACH_B200_ERR_DEVICE,
-                            "%s is on CUDA device %d but the current device is %d", name, attr.device,
-                            device);
+                return fail(MACH_B200_ERR_DEVICE, "%s is on CUDA device %d but the current device is %d", name,
+                            attr.device, device);
             }
             *r = kOnDevice;
             return MACH_B200_OK;
@@ -90,48 +102,243 @@ int residency(const void* p, int device, Residency* r, const char* name) {
     }
 }
 
-struct LaunchPlan {
-    int shape;
-    int passes;
-    dim3 grid;
+// ---------------------------------------------------------------- per-device state
+
+constexpr int kMaxDevices = 64;
+
+struct DeviceState {
+    std::once_flag once;
+    cudaError_t init_error = cudaSuccess;
+    int* status = nullptr;  // device address of g_mach_b200_status
+};
+DeviceState g_devices[kMaxDevices];
+
+// First call on a device (that device current): look up the status word and keep the
+// stream-ordered pool's memory cached between calls.
+int device_state(int device, DeviceState** out) {
+    if (device < 0 || device >= kMaxDevices) return fail(MACH_B200_ERR_DEVICE, "device %d out of range", device);
+    DeviceState& d = g_devices[device];
+    std::call_once(d.once, [&d, device]() {
+        void* p = nullptr;
+        d.init_error = cudaGetSymbolAddress(&p, g_mach_b200_status);
+        d.status = static_cast<int*>(p);
+        if (d.init_error == cudaSuccess) {
+            cudaMemPool_t pool;
+            if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+                uint64_t keep = UINT64_MAX;
+                cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+            }
+        }
+    });
+    if (d.init_error != cudaSuccess) {
+        return fail(MACH_B200_ERR_CUDA, "device setup failed: %s", cudaGetErrorString(d.init_error));
+    }
+    *out = &d;
+    return MACH_B200_OK;
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, []() {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess) {
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+        }
+    });
+    return fn;
+}
+
+// ---------------------------------------------------------------- launch planning
+
+constexpr int kMaxTxChunk = 32;  // lane-voxel kernel: 32 x 128 voxels x 4 B = 16 KB of arrivals
+
+struct Plan {
+    LaunchPlan lp{};
+    StagedArgs st{};
+    bool staged = false;
 };
 
-LaunchPlan plan_launch(uint64_t n_vox, uint32_t n_frames) {
-    LaunchPlan p{};
-    if (n_frames <= 1) {
-        p.shape = kShapeOneFrame;
-        p.passes = 1;
-    } else if (n_frames <= 8) {
-        p.shape = kShapeFewFrames;
-        p.passes = static_cast<int>(n_frames);
-    } else if (n_frames <= 16) {
-        p.shape = kShapeHalfWarp;
-        p.passes = 1;
-    } else {
-        p.shape = kShapeWarp;
-        p.passes = static_cast<int>(std::min<uint32_t>(8, (n_frames + 31) / 32));
-    }
-    const ShapeInfo si = shape_info(p.shape);
-    const uint64_t vox_per_cta = static_cast<uint64_t>(kThreadsPerBlock / 32) * (32 / si.lpv);
-    p.grid.x = static_cast<unsigned>((n_vox + vox_per_cta - 1) / vox_per_cta);
-    const uint32_t frames_per_cta = static_cast<uint32_t>(si.lpv * p.passes);
-    p.grid.y = (n_frames + frames_per_cta - 1) / frames_per_cta;
-    p.grid.z = 1;
+int next_pow2(int x) {
+    int p = 1;
+    while (p < x) p <<= 1;
     return p;
 }
 
-cudaError_t dispatch(int storage, const DasArgs& a, int interp, const LaunchPlan& plan, cudaStream_t st) {
-    g_launches.fetch_add(1, std::memory_order_relaxed);
-    switch (storage) {
-        case kF32: return launch_das_gather<kF32>(a, interp, plan.shape, plan.grid, st);
-        case kC64: return launch_das_gather<kC64>(a, interp, plan.shape, plan.grid, st);
-        case kF16: return launch_das_gather<kF16>(a, interp, plan.shape, plan.grid, st);
-        case kCF16: return launch_das_gather<kCF16>(a, interp, plan.shape, plan.grid, st);
-        case kBF16: return launch_das_gather<kBF16>(a, interp, plan.shape, plan.grid, st);
-        case kCBF16: return launch_das_gather<kCBF16>(a, interp, plan.shape, plan.grid, st);
-        case kI16: return launch_das_gather<kI16>(a, interp, plan.shape, plan.grid, st);
-        default: return launch_das_gather<kCI16>(a, interp, plan.shape, plan.grid, st);
+// Tile extents for a voxel grid (fast axis first); the product is exactly 128.
+void choose_tile(const mach_b200_options& o, StagedArgs& st) {
+    const int slow = o.grid_shape[0], mid = o.grid_shape[1], fast = o.grid_shape[2];
+    st.grid_fast = fast;
+    st.grid_mid = mid;
+    st.grid_slow = slow;
+    if (mid <= 1) {  // 2-D grid: 8 along the contiguous axis x 16 across
+        st.tile_fast = 8;
+        st.tile_mid = 1;
+        st.tile_slow = 16;
+    } else {  // 3-D grid: 8 x 4 x 4
+        st.tile_fast = 8;
+        st.tile_mid = 4;
+        st.tile_slow = 4;
     }
+    st.tiles_fast = (fast + st.tile_fast - 1) / st.tile_fast;
+    st.tiles_mid = (mid + st.tile_mid - 1) / st.tile_mid;
+}
+
+bool grid_matches(const mach_b200_options& o, uint64_t n_vox) {
+    const int64_t a = o.grid_shape[0], b = o.grid_shape[1], c = o.grid_shape[2];
+    return a > 0 && b > 0 && c > 0 && static_cast<uint64_t>(a * b * c) == n_vox;
+}
+
+Plan plan_launch(int storage, uint64_t n_vox, uint32_t n_frames, uint32_t n_tx, const void* channel,
+                 bool channel_on_device, const mach_b200_options& o) {
+    Plan p;
+    const int esz = static_cast<int>(storage_bytes(storage));
+    const int vf = 8 / esz;
+    int kind = o.kernel;
+    // Host channel data is staged into fresh (aligned) device buffers.
+    const bool vec_ok =
+        n_frames % static_cast<uint32_t>(vf) == 0 && (!channel_on_device || reinterpret_cast<uintptr_t>(channel) % 8 == 0);
+    if (kind == MACH_B200_KERNEL_AUTO) {
+        kind = n_frames <= 8 ? MACH_B200_KERNEL_LANE_VOXEL : (vec_ok ? MACH_B200_KERNEL_STAGED : MACH_B200_KERNEL_WARP);
+    }
+    if (kind == MACH_B200_KERNEL_LANE_VOXEL && n_frames > 8) kind = MACH_B200_KERNEL_WARP;
+    if (kind == MACH_B200_KERNEL_STAGED && !vec_ok) kind = MACH_B200_KERNEL_WARP;
+
+    if (kind == MACH_B200_KERNEL_LANE_VOXEL) {
+        p.lp.kind = n_frames <= 1 ? kKindLaneVoxel1 : kKindLaneVoxelN;
+        p.lp.passes = static_cast<int>(n_frames);
+        const int chunk = o.tx_chunk > 0 ? o.tx_chunk : kMaxTxChunk;
+        const uint32_t chunks = std::max<uint32_t>(1u, (n_tx + chunk - 1) / chunk);
+        p.lp.tx_chunk = static_cast<int>(std::max<uint32_t>(1u, (n_tx + chunks - 1) / chunks));
+        p.lp.block = dim3(kLaneVoxelThreads, 1, 1);
+        p.lp.grid = dim3(static_cast<unsigned>((n_vox + kLaneVoxelThreads - 1) / kLaneVoxelThreads), 1, 1);
+        p.lp.smem = static_cast<size_t>(p.lp.tx_chunk) * kLaneVoxelThreads * sizeof(float);
+        return p;
+    }
+    if (kind == MACH_B200_KERNEL_STAGED) {
+        const int lanes_needed = static_cast<int>((n_frames + vf - 1) / vf);
+        int lv = o.lanes_per_voxel > 0 ? o.lanes_per_voxel : std::min(32, std::max(4, next_pow2(lanes_needed)));
+        if (lv != 4 && lv != 8 && lv != 16 && lv != 32) lv = 32;
+        const int fc = lv * vf;
+        int w = o.window_rows > 0 ? o.window_rows : (fc * esz >= 256 ? 64 : 128);
+        w = std::min(256, std::max(4, (w + 3) & ~3));  // multiple of 4 keeps both windows 128-byte aligned
+        p.staged = true;
+        p.lp.kind = kKindStaged;
+        p.lp.lanes_per_voxel = lv;
+        p.lp.block = dim3(kStagedThreads, 1, 1);
+        p.lp.tx_chunk = 1;
+        p.lp.passes = 1;
+        if (grid_matches(o, n_vox)) {
+            choose_tile(o, p.st);
+            const int64_t tiles = static_cast<int64_t>(p.st.tiles_fast) * p.st.tiles_mid *
+                                  ((o.grid_shape[0] + p.st.tile_slow - 1) / p.st.tile_slow);
+            p.lp.grid = dim3(static_cast<unsigned>(tiles), (n_frames + fc - 1) / fc, 1);
+        } else {
+            p.st.grid_fast = 0;
+            p.lp.grid =
+                dim3(static_cast<unsigned>((n_vox + kTileVoxels - 1) / kTileVoxels), (n_frames + fc - 1) / fc, 1);
+        }
+        p.st.window_rows = w;
+        // TMA needs a 16-byte aligned base and a row pitch that is a multiple of 16 bytes.
+        p.st.use_tma = ((!channel_on_device || reinterpret_cast<uintptr_t>(channel) % 16 == 0) &&
+                        (static_cast<uint64_t>(n_frames) * esz) % 16 == 0 && tensor_map_encoder() != nullptr)
+                           ? 1
+                           : 0;
+        p.lp.smem = staged_smem_bytes(w, fc, esz);
+        return p;
+    }
+    // warp-per-voxel multi-frame kernel (any frame count)
+    int lpv;
+    if (n_frames <= 16) {
+        p.lp.kind = kKindWarpHalf;
+        lpv = 16;
+        p.lp.passes = 1;
+    } else {
+        p.lp.kind = kKindWarp;
+        lpv = 32;
+        p.lp.passes = static_cast<int>(std::min<uint32_t>(8, (n_frames + 31) / 32));
+    }
+    const uint64_t vox_per_cta = static_cast<uint64_t>(kThreadsPerBlock / 32) * (32 / lpv);
+    p.lp.block = dim3(kThreadsPerBlock, 1, 1);
+    p.lp.grid.x = static_cast<unsigned>((n_vox + vox_per_cta - 1) / vox_per_cta);
+    const uint32_t frames_per_cta = static_cast<uint32_t>(lpv * p.lp.passes);
+    p.lp.grid.y = (n_frames + frames_per_cta - 1) / frames_per_cta;
+    p.lp.grid.z = 1;
+    p.lp.smem = 0;
+    p.lp.tx_chunk = 1;
+    return p;
+}
+
+// 2-D TMA view of one launch's channel data: inner dim = frames, outer = (tx, element, sample) rows.
+int encode_channel_map(CUtensorMap* map, int storage, const void* channel, uint64_t rows, uint32_t n_frames,
+                       int frame_chunk, int window_rows) {
+    const int esz = static_cast<int>(storage_bytes(storage));
+    const CUtensorMapDataType dt =
+        esz == 8 ? CU_TENSOR_MAP_DATA_TYPE_UINT64 : (esz == 4 ? CU_TENSOR_MAP_DATA_TYPE_UINT32 : CU_TENSOR_MAP_DATA_TYPE_UINT16);
+    const cuuint64_t dims[2] = {n_frames, rows};
+    const cuuint64_t strides[1] = {static_cast<cuuint64_t>(n_frames) * esz};
+    const cuuint32_t box[2] = {static_cast<cuuint32_t>(frame_chunk), static_cast<cuuint32_t>(window_rows)};
+    const cuuint32_t elem_strides[2] = {1, 1};
+    const CUresult r = tensor_map_encoder()(map, dt, 2, const_cast<void*>(channel), dims, strides, box, elem_strides,
+                                            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(MACH_B200_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", static_cast<int>(r));
+    return MACH_B200_OK;
+}
+
+cudaError_t dispatch(int storage, const DasArgs& a, int interp, const Plan& plan, const CUtensorMap& map,
+                     cudaStream_t st) {
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+#define MACH_B200_CASE(S)                                                              \
+    case S:                                                                             \
+        return plan.staged ? launch_das_staged<S>(a, plan.st, map, interp, plan.lp, st) \
+                           : launch_das<S>(a, interp, plan.lp, st);
+    switch (storage) {
+        MACH_B200_CASE(kF32)
+        MACH_B200_CASE(kC64)
+        MACH_B200_CASE(kF16)
+        MACH_B200_CASE(kCF16)
+        MACH_B200_CASE(kBF16)
+        MACH_B200_CASE(kCBF16)
+        MACH_B200_CASE(kI16)
+        default:
+            return plan.staged ? launch_das_staged<kCI16>(a, plan.st, map, interp, plan.lp, st)
+                               : launch_das<kCI16>(a, interp, plan.lp, st);
+    }
+#undef MACH_B200_CASE
+}
+
+// Launch transmits [0, a.n_tx) so that every launch's channel span stays below 2^31 samples
+// (32-bit offsets inside the kernels).  Later launches always accumulate.
+int dispatch_split(int storage, DasArgs a, int interp, const Plan& plan, cudaStream_t st) {
+    const size_t esz = storage_bytes(storage);
+    const int64_t per_tx = static_cast<int64_t>(a.n_rx) * a.row_stride;
+    const int64_t max_tx = std::max<int64_t>(1, ((int64_t{1} << 31) - 1) / std::max<int64_t>(per_tx, 1));
+    const char* ch = static_cast<const char*>(a.channel);
+    const float* arr = a.arrivals;
+    const int total = a.n_tx;
+    int t0 = 0;
+    do {
+        DasArgs b = a;
+        b.n_tx = static_cast<int32_t>(std::min<int64_t>(max_tx, total - t0));
+        b.channel = ch + static_cast<size_t>(t0) * per_tx * esz;
+        b.arrivals = arr + static_cast<int64_t>(t0) * a.n_vox;
+        b.accumulate = t0 == 0 ? a.accumulate : 1;
+        CUtensorMap map;
+        std::memset(&map, 0, sizeof(map));
+        if (plan.staged && plan.st.use_tma && b.n_tx > 0) {
+            const int fc = plan.lp.lanes_per_voxel * static_cast<int>(8 / esz);
+            const int rc = encode_channel_map(&map, storage, b.channel,
+                                              static_cast<uint64_t>(b.n_tx) * a.n_rx * a.n_samples, a.n_frames, fc,
+                                              plan.st.window_rows);
+            if (rc) return rc;
+        }
+        MACH_B200_CUDA_TRY(dispatch(storage, b, interp, plan, map, st));
+        t0 += static_cast<int>(max_tx);
+    } while (t0 < total);
+    return MACH_B200_OK;
 }
 
 // Stream-ordered device buffer released at scope exit (on the stream it was allocated on).
@@ -172,17 +379,31 @@ struct StreamHolder {
     }
 };
 
-int compound_impl(int32_t storage, const void* channel_data, const float* rx_coords_m,
-                  const float* scan_coords_m, const float* tx_wave_arrivals_s, void* out, uint32_t n_tx,
-                  uint32_t n_rx, uint32_t n_samples, uint64_t n_scan, uint32_t n_frames, float f_number,
-                  float rx_start_s, float sampling_freq_hz, float sound_speed_m_s, float modulation_freq_hz,
-                  float tukey_alpha, int32_t interp_type, float channel_scale, cudaStream_t stream,
-                  uint32_t flags) {
+// After a synchronous call that ran a kernel with bounded waits: report (and clear) a timeout.
+int check_status(DeviceState* dev, cudaStream_t stream) {
+    int status = 0;
+    MACH_B200_CUDA_TRY(cudaMemcpyAsync(&status, dev->status, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    MACH_B200_CUDA_TRY(cudaStreamSynchronize(stream));
+    if (status != 0) {
+        const int zero = 0;
+        MACH_B200_CUDA_TRY(cudaMemcpyAsync(dev->status, &zero, sizeof(int), cudaMemcpyHostToDevice, stream));
+        MACH_B200_CUDA_TRY(cudaStreamSynchronize(stream));
+        return fail(MACH_B200_ERR_CUDA, "a kernel wait timed out (status %d); the output is incomplete", status);
+    }
+    return MACH_B200_OK;
+}
+
+int compound_impl(int32_t storage, const void* channel_data, const float* rx_coords_m, const float* scan_coords_m,
+                  const float* tx_wave_arrivals_s, void* out, uint32_t n_tx, uint32_t n_rx, uint32_t n_samples,
+                  uint64_t n_scan, uint32_t n_frames, float f_number, float rx_start_s, float sampling_freq_hz,
+                  float sound_speed_m_s, float modulation_freq_hz, float tukey_alpha, int32_t interp_type,
+                  float channel_scale, cudaStream_t stream, const mach_b200_options& opt) {
     g_error.clear();
+    const uint32_t flags = opt.flags;
     if (storage < kF32 || storage > kCI16) return fail(MACH_B200_ERR_VALUE, "unknown storage code %d", storage);
     if (interp_type < kNearest || interp_type > kQuadratic) {
-        return fail(MACH_B200_ERR_VALUE, "interp_type must be 0 (NearestNeighbor), 1 (Linear) or 2 (Quadratic), got %d",
-                    interp_type);
+        return fail(MACH_B200_ERR_VALUE,
+                    "interp_type must be 0 (NearestNeighbor), 1 (Linear) or 2 (Quadratic), got %d", interp_type);
     }
     // Same range check and message as mach (src/mach/kernel.cu:745-748).
     if (!(tukey_alpha >= 0.0f && tukey_alpha <= 1.0f)) {
@@ -194,9 +415,14 @@ int compound_impl(int32_t storage, const void* channel_data, const float* rx_coo
     if (need_channel && (!channel_data || !rx_coords_m || !tx_wave_arrivals_s)) {
         return fail(MACH_B200_ERR_VALUE, "channel_data, rx_coords_m and tx_wave_arrivals_s must not be NULL");
     }
-    if (n_frames > 65535u * 256u) return fail(MACH_B200_ERR_VALUE, "n_frames %u is too large", n_frames);
-    // Sample indices are exact FP32 integers only up to 2^24 (the interpolation bounds rely on it).
-    if (n_samples > (1u << 24)) return fail(MACH_B200_ERR_VALUE, "n_samples %u exceeds 2^24", n_samples);
+    if (n_frames > 1000000u) return fail(MACH_B200_ERR_VALUE, "n_frames %u is too large (at most 1000000)", n_frames);
+    // Sample positions are rounded with FP32 adds that are exact below 2^22.
+    if (n_samples > (1u << 22)) return fail(MACH_B200_ERR_VALUE, "n_samples %u exceeds 2^22", n_samples);
+    // One transmit's channel data is addressed with 32-bit offsets.
+    if (static_cast<uint64_t>(n_rx) * n_samples * n_frames >= (uint64_t{1} << 31)) {
+        return fail(MACH_B200_ERR_VALUE, "one transmit holds %llu samples; at most 2^31 - 1 are supported",
+                    static_cast<unsigned long long>(static_cast<uint64_t>(n_rx) * n_samples * n_frames));
+    }
     if (n_rx > 0x7fffffffu || n_tx > 0x7fffffffu) return fail(MACH_B200_ERR_VALUE, "n_rx / n_tx too large");
     if (n_scan > 0x7fffffffull * 4ull) {
         return fail(MACH_B200_ERR_VALUE, "n_scan %llu is too large", static_cast<unsigned long long>(n_scan));
@@ -204,8 +430,10 @@ int compound_impl(int32_t storage, const void* channel_data, const float* rx_coo
 
     int device = 0;
     MACH_B200_CUDA_TRY(cudaGetDevice(&device));
-    Residency r_ch = kOnDevice, r_rx = kOnDevice, r_scan = kOnDevice, r_arr = kOnDevice, r_out = kOnDevice;
+    DeviceState* dev = nullptr;
     int rc;
+    if ((rc = device_state(device, &dev))) return rc;
+    Residency r_ch = kOnDevice, r_rx = kOnDevice, r_scan = kOnDevice, r_arr = kOnDevice, r_out = kOnDevice;
     if (need_channel) {
         if ((rc = residency(channel_data, device, &r_ch, "channel_data"))) return rc;
         if ((rc = residency(rx_coords_m, device, &r_rx, "rx_coords_m"))) return rc;
@@ -240,8 +468,10 @@ int compound_impl(int32_t storage, const void* channel_data, const float* rx_coo
     a.apod = tukey_alpha > 0.0f;
     a.rotate = cplx && modulation_freq_hz != 0.0f;
     const bool overwrite = (flags & MACH_B200_FLAG_OVERWRITE) != 0u || r_out != kOnDevice;
-    const LaunchPlan plan = plan_launch(n_scan, n_frames);
-    a.frame_passes = plan.passes;
+    Plan plan = plan_launch(storage, n_scan, n_frames, n_tx, channel_data, r_ch == kOnDevice, opt);
+    plan.st.status = dev->status;
+    a.frame_passes = plan.lp.passes;
+    a.tx_chunk = plan.lp.tx_chunk;
 
     const bool all_device = r_ch == kOnDevice && r_rx == kOnDevice && r_scan == kOnDevice && r_arr == kOnDevice &&
                             r_out == kOnDevice;
@@ -251,8 +481,11 @@ int compound_impl(int32_t storage, const void* channel_data, const float* rx_coo
         a.out = out;
         a.n_tx = static_cast<int32_t>(need_channel ? n_tx : 0);
         a.accumulate = overwrite ? 0 : 1;
-        MACH_B200_CUDA_TRY(dispatch(storage, a, interp_type, plan, stream));
-        if (!(flags & MACH_B200_FLAG_ASYNC)) MACH_B200_CUDA_TRY(cudaStreamSynchronize(stream));
+        if ((rc = dispatch_split(storage, a, interp_type, plan, stream))) return rc;
+        if (!(flags & MACH_B200_FLAG_ASYNC)) {
+            MACH_B200_CUDA_TRY(cudaStreamSynchronize(stream));
+            if (plan.staged) return check_status(dev, stream);
+        }
         return MACH_B200_OK;
     }
 
@@ -260,8 +493,8 @@ int compound_impl(int32_t storage, const void* channel_data, const float* rx_coo
     DeviceBuffer d_rx, d_scan, d_out, d_ch[2], d_arr[2];
     if (need_channel && r_rx != kOnDevice) {
         MACH_B200_CUDA_TRY(d_rx.alloc(static_cast<size_t>(n_rx) * 12, stream));
-        MACH_B200_CUDA_TRY(cudaMemcpyAsync(d_rx.ptr, rx_coords_m, static_cast<size_t>(n_rx) * 12,
-                                           cudaMemcpyHostToDevice, stream));
+        MACH_B200_CUDA_TRY(
+            cudaMemcpyAsync(d_rx.ptr, rx_coords_m, static_cast<size_t>(n_rx) * 12, cudaMemcpyHostToDevice, stream));
         a.rx = static_cast<const float*>(d_rx.ptr);
     }
     if (r_scan != kOnDevice) {
@@ -287,10 +520,14 @@ int compound_impl(int32_t storage, const void* channel_data, const float* rx_coo
         a.arrivals = tx_wave_arrivals_s;
         a.n_tx = static_cast<int32_t>(n_tx);
         a.accumulate = overwrite ? 0 : 1;
-        MACH_B200_CUDA_TRY(dispatch(storage, a, interp_type, plan, stream));
+        if ((rc = dispatch_split(storage, a, interp_type, plan, stream))) return rc;
     } else {
-        // Transmit chunks copied on a side stream while the previous chunk is gathered.
-        const uint32_t chunk = std::max<uint32_t>(1u, std::min<uint32_t>(n_tx, (n_tx + 7u) / 8u));
+        // Transmit chunks (>= 64 MB, at most 8 of them) copied on a side stream while the
+        // previous chunk is gathered.
+        const size_t target = size_t{64} << 20;
+        const uint32_t by_bytes = static_cast<uint32_t>(std::max<size_t>(1, target / std::max<size_t>(tx_bytes, 1)));
+        const uint32_t chunk =
+            std::max<uint32_t>(1u, std::min<uint32_t>(n_tx, std::max<uint32_t>(by_bytes, (n_tx + 7u) / 8u)));
         StreamHolder copy;
         EventPair copied, consumed;
         MACH_B200_CUDA_TRY(cudaStreamCreateWithFlags(&copy.s, cudaStreamNonBlocking));
@@ -331,18 +568,25 @@ int compound_impl(int32_t storage, const void* channel_data, const float* rx_coo
             MACH_B200_CUDA_TRY(cudaStreamWaitEvent(stream, copied.ev[b], 0));
             a.n_tx = static_cast<int32_t>(nt);
             a.accumulate = (k > 0 || !overwrite) ? 1 : 0;
-            MACH_B200_CUDA_TRY(dispatch(storage, a, interp_type, plan, stream));
+            if ((rc = dispatch_split(storage, a, interp_type, plan, stream))) return rc;
             MACH_B200_CUDA_TRY(cudaEventRecord(consumed.ev[b], stream));
         }
-        // Later frees on `stream` must wait for the copy stream's last use of the buffers.
-        MACH_B200_CUDA_TRY(cudaStreamWaitEvent(stream, copied.ev[(k - 1) & 1u], 0));
     }
     if (r_out != kOnDevice) {
         MACH_B200_CUDA_TRY(cudaMemcpyAsync(out, dev_out, out_bytes, cudaMemcpyDeviceToHost, stream));
     }
     // Host buffers are in use until the stream drains: always synchronous here.
     MACH_B200_CUDA_TRY(cudaStreamSynchronize(stream));
+    if (plan.staged) return check_status(dev, stream);
     return MACH_B200_OK;
+}
+
+mach_b200_options default_options(uint32_t flags) {
+    mach_b200_options o;
+    std::memset(&o, 0, sizeof(o));
+    o.struct_size = sizeof(o);
+    o.flags = flags;
+    return o;
 }
 
 }  // namespace
@@ -356,7 +600,7 @@ int mach_b200_beamform_f32(const float* channel_data, const float* rx_coords_m, 
                            float tukey_alpha, int32_t interp_type) {
     return compound_impl(kF32, channel_data, rx_coords_m, scan_coords_m, tx_wave_arrivals_s, out, 1u, n_rx,
                          n_samples, n_scan, n_frames, f_number, rx_start_s, sampling_freq_hz, sound_speed_m_s,
-                         modulation_freq_hz, tukey_alpha, interp_type, 1.0f, nullptr, 0u);
+                         modulation_freq_hz, tukey_alpha, interp_type, 1.0f, nullptr, default_options(0u));
 }
 
 int mach_b200_beamform_c64(const void* channel_data, const float* rx_coords_m, const float* scan_coords_m,
@@ -366,7 +610,7 @@ int mach_b200_beamform_c64(const void* channel_data, const float* rx_coords_m, c
                            float tukey_alpha, int32_t interp_type) {
     return compound_impl(kC64, channel_data, rx_coords_m, scan_coords_m, tx_wave_arrivals_s, out, 1u, n_rx,
                          n_samples, n_scan, n_frames, f_number, rx_start_s, sampling_freq_hz, sound_speed_m_s,
-                         modulation_freq_hz, tukey_alpha, interp_type, 1.0f, nullptr, 0u);
+                         modulation_freq_hz, tukey_alpha, interp_type, 1.0f, nullptr, default_options(0u));
 }
 
 int mach_b200_beamform_compound(int32_t storage, const void* channel_data, const float* rx_coords_m,
@@ -378,7 +622,27 @@ int mach_b200_beamform_compound(int32_t storage, const void* channel_data, const
     return compound_impl(storage, channel_data, rx_coords_m, scan_coords_m, tx_wave_arrivals_s, out, n_tx, n_rx,
                          n_samples, n_scan, n_frames, f_number, rx_start_s, sampling_freq_hz, sound_speed_m_s,
                          modulation_freq_hz, tukey_alpha, interp_type, channel_scale,
-                         static_cast<cudaStream_t>(cuda_stream), flags);
+                         static_cast<cudaStream_t>(cuda_stream), default_options(flags));
+}
+
+int mach_b200_beamform_ex(int32_t storage, const void* channel_data, const float* rx_coords_m,
+                          const float* scan_coords_m, const float* tx_wave_arrivals_s, void* out, uint32_t n_tx,
+                          uint32_t n_rx, uint32_t n_samples, uint64_t n_scan, uint32_t n_frames, float f_number,
+                          float rx_start_s, float sampling_freq_hz, float sound_speed_m_s, float modulation_freq_hz,
+                          float tukey_alpha, int32_t interp_type, float channel_scale, void* cuda_stream,
+                          const mach_b200_options* options) {
+    mach_b200_options o = default_options(0u);
+    if (options) {
+        if (options->struct_size < offsetof(mach_b200_options, reserved)) {
+            g_error = "mach_b200_options.struct_size is too small";
+            return MACH_B200_ERR_VALUE;
+        }
+        std::memcpy(&o, options, std::min<size_t>(sizeof(o), options->struct_size));
+    }
+    return compound_impl(storage, channel_data, rx_coords_m, scan_coords_m, tx_wave_arrivals_s, out, n_tx, n_rx,
+                         n_samples, n_scan, n_frames, f_number, rx_start_s, sampling_freq_hz, sound_speed_m_s,
+                         modulation_freq_hz, tukey_alpha, interp_type, channel_scale,
+                         static_cast<cudaStream_t>(cuda_stream), o);
 }
 
 const char* mach_b200_last_error(void) { return g_error.c_str(); }

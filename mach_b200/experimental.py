@@ -15,7 +15,7 @@ from __future__ import annotations
 import warnings
 from typing import Any
 
-from mach_b200 import _cuda_impl, _dlpack
+from mach_b200 import _cuda_impl, _dlpack, _grid
 from mach_b200._array_api import array_namespace, is_writeable_array
 from mach_b200._check import ensure_contiguous, is_contiguous
 from mach_b200._cuda_impl import InterpolationType
@@ -45,6 +45,11 @@ def beamform(
     interp_type: InterpolationType = InterpolationType.Linear,
     channel_scale: float = 1.0,
     sync: bool = True,
+    grid_shape: Any = None,
+    kernel: str = "auto",
+    window_rows: int = 0,
+    lanes_per_voxel: int = 0,
+    tx_chunk: int = 0,
 ) -> Any:
     """Beamform and coherently compound ``n_transmits`` transmits.
 
@@ -57,6 +62,11 @@ def beamform(
         channel_scale: multiplier applied to every sample (for int16 storage).
         sync: when False and every array is on the GPU, return without waiting for the
             kernel (it runs on the current torch stream for torch inputs).
+        grid_shape: ``(slow, mid, fast)`` extents when ``scan_coords_m`` is a flattened grid
+            (fast = contiguous axis); ``None`` detects it, ``False`` disables tiling by grid.
+            Only the voxel-to-CTA assignment depends on it, never the result.
+        kernel, window_rows, lanes_per_voxel, tx_chunk: launch tuning (see
+            ``mach_b200_options`` in include/mach_b200.h); the autotuner sets them.
         Other arguments as in :func:`mach_b200.kernel.beamform`.
 
     Returns:
@@ -126,11 +136,16 @@ def beamform(
         )
     all_gpu = all(v.on_cuda for v in (ch, rx, scan, arr, o))
     flags = 0 if (sync or not all_gpu) else _cuda_impl.FLAG_ASYNC
+    if grid_shape is None:
+        grid_shape = _grid.detect(scan_coords_m)
+    options = _cuda_impl.make_options(
+        flags, grid_shape=grid_shape or None, kernel=kernel, tx_chunk=tx_chunk, window_rows=window_rows,
+        lanes_per_voxel=lanes_per_voxel)
     _cuda_impl.beamform_compound(
         ch, storage, rx, scan, arr, o, n_tx=n_tx, n_rx=n_rx, n_samples=n_samples, n_vox=n_points,
         n_frames=n_frames, f_number=f_number, rx_start_s=rx_start_s, sampling_freq_hz=sampling_freq_hz,
         sound_speed_m_s=sound_speed_m_s, modulation_freq_hz=modulation_freq_hz, tukey_alpha=tukey_alpha,
         interp_type=int(interp_type), channel_scale=channel_scale, stream=_current_stream(channel_data),
-        flags=flags,
+        flags=flags, options=options,
     )
     return out

@@ -80,3 +80,14 @@ def test_contiguity_helpers():
     with pytest.warns(UserWarning, match="array is not contiguous"):
         fixed = _check.ensure_contiguous(arr.T)
     assert fixed.flags["C_CONTIGUOUS"]
+
+
+def test_grid_hint_detection():
+    from mach_b200 import _grid
+    from tests import _helpers as H
+
+    w = H.small("doppler", n_x=10, n_z=24)
+    assert _grid.detect(w.scan_coords_m) == (10, 1, 24)
+    w3 = H.small("volume3d", n_side=8)
+    assert _grid.detect(w3.scan_coords_m) == (8, 8, 8)
+    assert _grid.detect(np.random.default_rng(0).normal(size=(50, 3)).astype(np.float32)) is None

@@ -1,0 +1,90 @@
+"""Every kernel family computes the same sums: staged-window (TMA and direct loads),
+warp-per-voxel and voxel-per-lane, for every storage type and interpolation, with and
+without a voxel-grid tiling hint; each is also checked against the FP64 oracle."""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from tests import _helpers as H
+
+pytestmark = pytest.mark.gpu
+
+STORAGES = ["f32", "c64", "f16", "cf16", "bf16", "cbf16", "i16", "ci16"]
+
+
+def _workload(storage: str, n_frames: int, interp: int):
+    """Small multi-frame job in the requested storage (complex ones from the Doppler physics)."""
+    import torch
+
+    if storage in ("c64", "cf16", "cbf16", "ci16"):
+        w = H.small("doppler", n_x=10, n_z=24, n_tx=2, n_frames=n_frames, n_elements=48)
+        ch = w.channel
+        if storage == "cf16":
+            ch = torch.view_as_real(ch).to(torch.float16).contiguous()
+        elif storage == "cbf16":
+            ch = torch.view_as_real(ch).to(torch.bfloat16).contiguous()
+        elif storage == "ci16":
+            scale = float(torch.view_as_real(ch).abs().max()) / 20000.0
+            ch = (torch.view_as_real(ch) / scale).round().to(torch.int16).contiguous()
+            w.channel_scale = scale
+    else:
+        w = H.small("volume3d", n_side=6, n_elem_side=8, n_frames=n_frames, n_samples=1400)
+        ch = w.channel
+        if storage == "f32":
+            ch = ch.to(torch.float32) * w.channel_scale
+            w.channel_scale = 1.0
+        elif storage in ("f16", "bf16"):
+            ch = (ch.to(torch.float32) * w.channel_scale).to(torch.float16 if storage == "f16" else torch.bfloat16)
+            w.channel_scale = 1.0
+    w.channel = ch.contiguous()
+    w.storage = storage
+    w.params["interp_type"] = interp
+    return w
+
+
+def _run(w, **kw):
+    return H.gpu_compound(w, **kw)
+
+
+@pytest.mark.parametrize("storage", STORAGES)
+@pytest.mark.parametrize("interp", [0, 1, 2])
+def test_staged_matches_warp_kernel_and_oracle(cuda, storage, interp):
+    w = _workload(storage, 16, interp)
+    staged = _run(w, kernel="staged")
+    warp = _run(w, kernel="warp")
+    direct = _run(w, kernel="staged", window_rows=4)  # windows never fit: taps from global memory
+    flat = _run(w, kernel="staged", grid_shape=False)  # 1-D tiles
+    assert np.abs(staged).max() > 0
+    for other in (warp, direct, flat):
+        assert H.rel_l2(staged, other) <= 2e-6
+    db = H.nrms_db(staged, H.oracle(w, storage=storage))
+    assert db <= -60.0, f"{storage}: {db:.1f} dB vs the oracle on the stored samples"
+
+
+@pytest.mark.parametrize("n_frames", [9, 12, 16, 24, 32, 40, 64, 72])
+def test_staged_frame_chunks(cuda, n_frames):
+    w = _workload("c64", n_frames, 1)
+    staged = _run(w, kernel="staged")
+    warp = _run(w, kernel="warp")
+    assert H.rel_l2(staged, warp) <= 2e-6
+
+
+@pytest.mark.parametrize("lanes", [4, 8, 16, 32])
+@pytest.mark.parametrize("window_rows", [16, 64, 256])
+def test_staged_tuning_knobs_do_not_change_results(cuda, lanes, window_rows):
+    w = _workload("cf16", 32, 2)
+    base = _run(w, kernel="warp")
+    got = _run(w, kernel="staged", lanes_per_voxel=lanes, window_rows=window_rows)
+    assert H.rel_l2(got, base) <= 2e-6
+
+
+@pytest.mark.parametrize("storage", STORAGES)
+@pytest.mark.parametrize("n_frames", [1, 3])
+def test_lane_voxel_storage(cuda, storage, n_frames):
+    w = _workload(storage, n_frames, 2)
+    got = _run(w)
+    tuned = _run(w, tx_chunk=1)  # transmit-major summation order: FP32 rounding only
+    assert H.rel_l2(got, tuned) <= 1e-5
+    assert H.nrms_db(got, H.oracle(w, storage=storage)) <= -60.0
