@@ -182,9 +182,12 @@ def make_workload(name: str, frames: int | None = None):
 
 
 def storage_channel(w, storage):
+    """Channel data in the requested storage; sets ``w.storage_scale`` for int16."""
     from mach_b200 import workloads as W
 
-    return W.to_storage(w, storage).contiguous()
+    ch, scale = W.as_storage(w, storage)
+    w.storage_scale = scale
+    return ch.contiguous()
 
 
 def algorithmic_bytes(w, storage) -> int:
@@ -215,7 +218,7 @@ def run_ours(args, world, rank, local):
     common = dict(n_tx=w.n_tx, n_rx=w.n_rx, n_samples=w.n_samples, n_vox=w.n_vox, n_frames=w.n_frames,
                   f_number=p["f_number"], rx_start_s=p["rx_start_s"], sampling_freq_hz=p["sampling_freq_hz"],
                   sound_speed_m_s=p["sound_speed_m_s"], modulation_freq_hz=p["modulation_freq_hz"],
-                  tukey_alpha=p["tukey_alpha"], interp_type=p["interp_type"], channel_scale=w.channel_scale)
+                  tukey_alpha=p["tukey_alpha"], interp_type=p["interp_type"], channel_scale=w.storage_scale)
 
     from mach_b200 import _grid
 
@@ -304,19 +307,19 @@ def accuracy_and_baselines(args, w, storage, result):
     p = {k: w.params[k] for k in keys}
     cores = os.cpu_count() or 1
 
-    def oracle_on(n_sub, data, st):
+    def oracle_on(n_sub, data, st, scale):
         sel = np.unique(np.linspace(0, w.n_vox - 1, n_sub).astype(np.int64))
         t = time.perf_counter()
         y = oracle_c.beamform_c(data, w.rx_coords_m, w.scan_coords_m, w.tx_wave_arrivals_s, storage=st,
-                                channel_scale=w.channel_scale, voxel_subset=sel, n_threads=cores, **p)
+                                channel_scale=scale, voxel_subset=sel, n_threads=cores, **p)
         return sel, y, time.perf_counter() - t
 
     n_sub = 256
-    sel, y, dt = oracle_on(n_sub, ch_np, storage)
+    sel, y, dt = oracle_on(n_sub, ch_np, storage, w.storage_scale)
     if not args.no_cpu_baseline:
         while dt < 0.25 * args.cpu_seconds and n_sub < w.n_vox:
             n_sub = int(min(w.n_vox, n_sub * max(2.0, 0.5 * args.cpu_seconds / max(dt, 1e-3))))
-            sel, y, dt = oracle_on(n_sub, ch_np, storage)
+            sel, y, dt = oracle_on(n_sub, ch_np, storage, w.storage_scale)
         pts = len(sel) * w.n_rx * w.n_tx * w.n_frames
         extra["cpu_baseline"] = {
             "value": pts / dt, "unit": "points/s", "cores": cores, "kind": "port",
@@ -326,7 +329,7 @@ def accuracy_and_baselines(args, w, storage, result):
     got = result.cpu().numpy()[sel]
     acc = {"nrms_db_vs_fp64_oracle_on_stored_samples": das_fp64.nrms_db(got, y), "oracle_voxels": int(len(sel))}
     if storage != w.storage:
-        _, y_src, _ = oracle_on(len(sel), src_np, w.storage)
+        _, y_src, _ = oracle_on(len(sel), src_np, w.storage, w.channel_scale)
         acc["nrms_db_vs_fp64_oracle_on_source_data"] = das_fp64.nrms_db(got, y_src)
     if machref.available() and w.storage in ("c64", "f32", "i16"):
         ref = reference_once(w)
@@ -336,7 +339,9 @@ def accuracy_and_baselines(args, w, storage, result):
 
 
 def storage_numpy(w, storage):
-    ch = storage_channel(w, storage)
+    from mach_b200 import workloads as W
+
+    ch, _ = W.as_storage(w, storage)
     if ch.dtype == torch.bfloat16:
         return ch.view(torch.int16).cpu().numpy().view(np.uint16)
     return ch.cpu().numpy()
@@ -378,7 +383,7 @@ def run_e2e(args, w, storage, ch_dev, world, local):
     def step():
         with warnings.catch_warnings():
             warnings.simplefilter("ignore", UserWarning)
-            experimental.beamform(ch_h, rx_h, scan_h, arr_h, out=out_h, channel_scale=w.channel_scale, **w.params)
+            experimental.beamform(ch_h, rx_h, scan_h, arr_h, out=out_h, channel_scale=w.storage_scale, **w.params)
 
     for _ in range(max(1, min(args.warmup, 3))):
         step()

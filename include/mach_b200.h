@@ -59,12 +59,17 @@ extern "C" {
 /* Flags for mach_b200_beamform_compound / mach_b200_beamform_ex. */
 #define MACH_B200_FLAG_ASYNC 1u     /* return without synchronising `cuda_stream` (device buffers only) */
 #define MACH_B200_FLAG_OVERWRITE 2u /* out = result instead of out += result */
+#define MACH_B200_FLAG_SPLIT_DELAY 4u /* sample positions and phases formed in FP64 per receive path and
+                                         per transmit, combined as integer base + FP32 fraction (more
+                                         accurate than mach's FP32 delay; not bit-identical to mach) */
 
 /* Kernel families (mach_b200_options.kernel). */
 #define MACH_B200_KERNEL_AUTO 0
 #define MACH_B200_KERNEL_LANE_VOXEL 1 /* one lane per voxel, all frames in registers (1..8 frames) */
 #define MACH_B200_KERNEL_STAGED 2     /* voxel tiles, sample windows staged in shared memory by TMA */
 #define MACH_B200_KERNEL_WARP 3       /* a warp per voxel over frames, taps read from global memory */
+#define MACH_B200_KERNEL_ENSEMBLE 4   /* lanes = frames of a 32-lane block, voxel-tile sample windows in
+                                         tensor memory (many frames; nearest or linear taps) */
 
 /*
  * Optional launch options.  Zero-initialise, set struct_size = sizeof(mach_b200_options),
@@ -78,7 +83,7 @@ typedef struct mach_b200_options {
                                flattened); zeros = no grid: tiles are runs of consecutive voxels */
     int32_t kernel;          /* MACH_B200_KERNEL_*, 0 = automatic */
     int32_t tx_chunk;        /* lane-voxel kernel: transmits per shared-memory pass, 0 = automatic */
-    int32_t window_rows;     /* staged kernel: sample rows per staged window, 0 = automatic */
+    int32_t window_rows;     /* staged / ensemble kernels: sample rows per window, 0 = automatic */
     int32_t lanes_per_voxel; /* staged kernel: 4, 8, 16 or 32, 0 = automatic */
     int32_t reserved[4];
 } mach_b200_options;
@@ -139,6 +144,50 @@ MACH_B200_API int mach_b200_beamform_ex(int32_t storage, const void* channel_dat
                                 float modulation_freq_hz, float tukey_alpha,
                                 int32_t interp_type, float channel_scale, void* cuda_stream,
                                 const mach_b200_options* options);
+
+/* One job of a batch: every pointer must be device memory of the current device. */
+typedef struct mach_b200_job {
+    int32_t storage;             /* MACH_B200_STORAGE_* */
+    int32_t interp_type;         /* MACH_B200_NEAREST / LINEAR / QUADRATIC */
+    const void* channel_data;    /* [n_tx][n_rx][n_samples][n_frames] */
+    const float* rx_coords_m;    /* [n_rx][3] */
+    const float* scan_coords_m;  /* [n_scan][3] */
+    const float* tx_wave_arrivals_s; /* [n_tx][n_scan] */
+    void* out;                   /* [n_scan][n_frames] */
+    uint32_t n_tx, n_rx, n_samples, n_frames;
+    uint64_t n_scan;
+    float f_number, rx_start_s, sampling_freq_hz, sound_speed_m_s, modulation_freq_hz, tukey_alpha;
+    float channel_scale;
+    uint32_t flags;              /* MACH_B200_FLAG_OVERWRITE, MACH_B200_FLAG_SPLIT_DELAY */
+    int32_t grid_shape[3];       /* as in mach_b200_options */
+    int32_t kernel;              /* tuning knobs as in mach_b200_options (0 = automatic);      */
+    int32_t tx_chunk;            /* MACH_B200_KERNEL_WARP is not available in batches          */
+    int32_t window_rows;
+    int32_t lanes_per_voxel;
+} mach_b200_job;
+
+/* Reusable batch context: pinned host and device job tables, work counters. */
+typedef struct mach_b200_batch mach_b200_batch;
+
+/* Create a context for batches of up to max_jobs jobs on the current device. */
+MACH_B200_API int mach_b200_batch_create(uint32_t max_jobs, mach_b200_batch** batch);
+
+/*
+ * Beamform a batch of device-resident jobs with one persistent launch per kernel
+ * signature (storage, interpolation, kernel family): the resident CTAs pull (job, tile)
+ * work items from a device counter until every tile of every job is done, so jobs of
+ * different grid sizes, transmit and frame counts share the GPU.  Only asynchronous
+ * copies (job table, from the context's pinned buffer), memsets and launches are
+ * enqueued on `cuda_stream`, so the call can be captured in a CUDA graph and replayed
+ * (replays reuse the captured job table).  mach has no batch interface (its call
+ * beamforms one transmit of one job), so this entry point has no counterpart there.
+ * `flags`: MACH_B200_FLAG_ASYNC to return without synchronising.
+ */
+MACH_B200_API int mach_b200_batch_run(mach_b200_batch* batch, const mach_b200_job* jobs, uint32_t n_jobs,
+                                      void* cuda_stream, uint32_t flags);
+
+/* Release a batch context (waits for its device work to finish). */
+MACH_B200_API void mach_b200_batch_destroy(mach_b200_batch* batch);
 
 /* Message of the last failed call on this thread ("" if none). */
 MACH_B200_API const char* mach_b200_last_error(void);

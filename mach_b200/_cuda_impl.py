@@ -58,7 +58,7 @@ class Options(ctypes.Structure):
     ]
 
 
-KERNELS = {"auto": 0, "lane_voxel": 1, "staged": 2, "warp": 3}
+KERNELS = {"auto": 0, "lane_voxel": 1, "staged": 2, "warp": 3, "ensemble": 4}
 
 
 def make_options(flags: int = 0, grid_shape=None, kernel: str | int = 0, tx_chunk: int = 0, window_rows: int = 0,
@@ -91,6 +91,7 @@ library_path: str = str(_LIB_PATH)
 
 FLAG_ASYNC = 1
 FLAG_OVERWRITE = 2
+FLAG_SPLIT_DELAY = 4
 
 STORAGE_CODES = {"f32": 0, "c64": 1, "f16": 2, "cf16": 3, "bf16": 4, "cbf16": 5, "i16": 6, "ci16": 7}
 
@@ -292,7 +293,7 @@ def beamform_compound(
     if options is None:
         options = make_options(flags)
     else:
-        options.flags = int(flags)
+        options.flags = int(options.flags) | int(flags)
     rc = _lib.mach_b200_beamform_ex(
         STORAGE_CODES[storage], channel.ptr, rx.ptr, scan.ptr, arrivals.ptr, out.ptr, n_tx, n_rx, n_samples,
         n_vox, n_frames, float(f_number), float(rx_start_s), float(sampling_freq_hz), float(sound_speed_m_s),

@@ -126,7 +126,38 @@ struct DasArgs {
     int32_t accumulate;     // out += result (reference semantics) instead of out = result
     int32_t frame_passes;   // frames handled per lane (multi-frame kernel)
     int32_t tx_chunk;       // transmits whose arrivals are staged in shared memory at once
+    // Split-delay mode: sample positions and phases formed in FP64 per (voxel, element) and
+    // per (voxel, transmit), each split into an integer sample base + FP32 fraction.
+    int32_t split;
+    int32_t start_base;     // floor(-t0 * fs): samples before it belong to tau < 0
+    float start_frac;       // -t0 * fs - start_base
+    double fs_d;            // sampling frequency
+    double t0_d;            // rx_start_s
+    double fmod_d;          // modulation frequency
+    double fs_over_c;       // fs / c
+    double fmod_over_c;     // f_mod / c
 };
+
+// Integer base + FP32 fraction in [0, 1) of a non-negative-or-negative FP64 sample position.
+struct SplitPos {
+    int base;
+    float frac;
+};
+
+__device__ __forceinline__ SplitPos split_position(double s) {
+    const double b = floor(s);
+    SplitPos p{static_cast<int>(b), static_cast<float>(s - b)};
+    if (p.frac >= 1.0f) {  // s - b rounded up to 1.0f
+        p.frac = 0.0f;
+        p.base += 1;
+    }
+    return p;
+}
+
+// Fractional revolutions in [-0.5, 0.5] of an FP64 phase measured in cycles.
+__device__ __forceinline__ float reduced_cycles(double cycles) {
+    return static_cast<float>(cycles - rint(cycles));
+}
 
 // Half-Tukey weight of r = horizontal distance / aperture radius (kernel.cu:333-349).
 __device__ __forceinline__ float tukey_weight(float r, float alpha, float one_minus_alpha) {

@@ -18,7 +18,7 @@
 //     once -- no atomics, no second pass.
 #pragma once
 
-#include "das_device.cuh"
+#include "das_lane_voxel.cuh"
 
 namespace mach_b200 {
 
@@ -105,12 +105,10 @@ __global__ void __launch_bounds__(kThreadsPerBlock) das_gather_kernel(const __gr
                 // Receive path of this lane's pair (voxel g, element eb + c0 + sub).
                 const int pe = eb + c0 + sub;
                 bool pair_ok = vox_ok && pe < a.n_rx && ((chunk_mask >> sub) & 1u);
-                float dist = 0.f, weight = 0.f;
+                PairRx rx{};
                 if (pair_ok) {
-                    bool in_ap;
-                    receive_path(a, __ldg(a.rx + 3 * pe + 0), __ldg(a.rx + 3 * pe + 1), __ldg(a.rx + 3 * pe + 2),
-                                 vx, vy, vz, radius, radius_sq, dist, weight, in_ap);
-                    pair_ok = in_ap && !(weight == 0.0f);  // kernel.cu:634 (tau = -1 marks outside)
+                    pair_ok = pair_receive(a, __ldg(a.rx + 3 * pe + 0), __ldg(a.rx + 3 * pe + 1),
+                                           __ldg(a.rx + 3 * pe + 2), vx, vy, vz, radius, radius_sq, rx);
                 }
                 const bool any_pair = __any_sync(kFull, pair_ok);
                 if (!any_pair) continue;
@@ -119,23 +117,9 @@ __global__ void __launch_bounds__(kThreadsPerBlock) das_gather_kernel(const __gr
                 for (int j = 0; j < kTxGroup; ++j) {
                     const int tx = tg + j;
                     if (tx >= a.n_tx) continue;
-                    float s = 0.f, cw = 0.f, sw = 0.f;
-                    bool ok = false;
-                    if (pair_ok) {
-                        float tau;
-                        ok = sample_position<INTERP>(a, dist, txa[j], tau, s);
-                        if (ok) {
-                            const float w = __fmul_rn(weight, a.scale);
-                            if (kCplx && a.rotate) {
-                                float sn, cs;
-                                __sincosf(__fmul_rn(a.mod_rad, tau), &sn, &cs);  // kernel.cu:656-658
-                                cw = __fmul_rn(cs, w);
-                                sw = __fmul_rn(sn, w);
-                            } else {
-                                cw = w;
-                            }
-                        }
-                    }
+                    int idx = 0;
+                    float w = 0.f, cw = 0.f, sw = 0.f;
+                    const bool ok = pair_ok && point_taps<INTERP, kCplx>(a, rx, txa[j], idx, w, cw, sw);
                     const T* const tx_base = channel + static_cast<int64_t>(tx) * a.n_rx * a.row_stride;
 
                     if constexpr (LPV == 1) {
@@ -144,7 +128,7 @@ __global__ void __launch_bounds__(kThreadsPerBlock) das_gather_kernel(const __gr
 #pragma unroll
                             for (int p = 0; p < MAXP; ++p) {
                                 if (p < passes && frame0 + p < n_frames) {
-                                    const float2 x = interpolate<S, INTERP>(row + frame0 + p, s, n_frames);
+                                    const float2 x = gather_taps<S, INTERP>(row + frame0 + p, idx, w, n_frames);
                                     if constexpr (kCplx) {
                                         acc[p].x = __fmaf_rn(x.x, cw, __fmaf_rn(-x.y, sw, acc[p].x));
                                         acc[p].y = __fmaf_rn(x.y, cw, __fmaf_rn(x.x, sw, acc[p].y));
@@ -163,7 +147,8 @@ __global__ void __launch_bounds__(kThreadsPerBlock) das_gather_kernel(const __gr
                         while (kmask) {
                             const int k = __ffs(kmask) - 1;
                             kmask &= kmask - 1u;
-                            const float sk = __shfl_sync(kFull, s, k, LPV);
+                            const int idxk = __shfl_sync(kFull, idx, k, LPV);
+                            const float wk = __shfl_sync(kFull, w, k, LPV);
                             const float cwk = __shfl_sync(kFull, cw, k, LPV);
                             const float swk = kCplx ? __shfl_sync(kFull, sw, k, LPV) : 0.f;
                             const bool okk = (vmask >> (g * LPV + k)) & 1u;
@@ -173,7 +158,7 @@ __global__ void __launch_bounds__(kThreadsPerBlock) das_gather_kernel(const __gr
                                 for (int p = 0; p < MAXP; ++p) {
                                     const int f = frame0 + p * LPV;
                                     if (p < passes && f < n_frames) {
-                                        const float2 x = interpolate<S, INTERP>(row + f, sk, n_frames);
+                                        const float2 x = gather_taps<S, INTERP>(row + f, idxk, wk, n_frames);
                                         if constexpr (kCplx) {
                                             acc[p].x = __fmaf_rn(x.x, cwk, __fmaf_rn(-x.y, swk, acc[p].x));
                                             acc[p].y = __fmaf_rn(x.y, cwk, __fmaf_rn(x.x, swk, acc[p].y));

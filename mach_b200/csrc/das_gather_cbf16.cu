@@ -6,4 +6,8 @@ namespace mach_b200 {
 template cudaError_t launch_das<kCBF16>(const DasArgs&, int, const LaunchPlan&, cudaStream_t);
 template cudaError_t launch_das_staged<kCBF16>(const DasArgs&, const StagedArgs&, const CUtensorMap&, int,
                                              const LaunchPlan&, cudaStream_t);
+template cudaError_t launch_lane_voxel_persistent<kCBF16>(int, int, bool, const PersistentLaunch&, cudaStream_t);
+template cudaError_t launch_staged_persistent<kCBF16>(int, int, const PersistentLaunch&, cudaStream_t);
+template cudaError_t launch_das_ensemble<kCBF16>(const DasArgs&, const StagedArgs&, const EnsembleArgs&,
+                                               const CUtensorMap&, int, size_t, cudaStream_t);
 }  // namespace mach_b200

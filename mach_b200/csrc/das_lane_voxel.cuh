@@ -57,6 +57,41 @@ __device__ __forceinline__ TapPosition tap_position(float s) {
     return p;
 }
 
+// Split-delay sample position: base + frac with frac in [0, 1).  Applies mach's bounds
+// (kernel.cu:117, 156, 208) to s = base + frac exactly and rounds half to even.
+template <int INTERP>
+__device__ __forceinline__ bool split_tap_position(int base, float frac, int n_samples, TapPosition& tp) {
+    if constexpr (INTERP == kLinear) {
+        if (base < 0 || base > n_samples - 1 || (base == n_samples - 1 && frac != 0.0f)) return false;
+        tp.idx = base;
+        tp.w0 = frac;
+        tp.step = frac > 0.0f ? 1 : 0;
+        return true;
+    } else {
+        const int up = (frac > 0.5f || (frac == 0.5f && (base & 1))) ? 1 : 0;
+        tp.idx = base + up;
+        if constexpr (INTERP == kNearest) {
+            return tp.idx >= 0 && tp.idx < n_samples;
+        } else {
+            if (base < 1 || base > n_samples - 2 || (base == n_samples - 2 && frac != 0.0f)) return false;
+            const float x = __fsub_rn(frac, static_cast<float>(up));  // exact
+            const float hx = __fmul_rn(0.5f, x);
+            const float q = __fmul_rn(hx, x);
+            tp.w0 = __fsub_rn(q, hx);
+            tp.w1 = __fmaf_rn(-2.0f, q, 1.0f);
+            tp.w2 = __fadd_rn(q, hx);
+            return true;
+        }
+    }
+}
+
+// Phase of a split-delay point: cycles in [-1, 1] reduced to [-0.5, 0.5], then the fast
+// sincos on an argument within [-pi, pi] (its accurate range).
+__device__ __forceinline__ void split_phasor(float cycles, float& sn, float& cs) {
+    const float whole = __fsub_rn(__fadd_rn(cycles, kRoundMagic), kRoundMagic);
+    __sincosf(__fmul_rn(__fsub_rn(cycles, whole), 6.28318530717958647f), &sn, &cs);
+}
+
 // Interpolated sample at `row[idx * stride]` (stride = frames), widened to FP32.
 template <int S, int INTERP>
 __device__ __forceinline__ float2 tap_value(const typename Storage<S>::T* p, const TapPosition& tp, int stride) {
@@ -81,6 +116,76 @@ __device__ __forceinline__ float2 tap_value(const typename Storage<S>::T* p, con
     }
 }
 
+// ---- vectorised frames (NF frames contiguous per sample, 16-byte aligned rows) ----
+
+// float2 pairs holding NF frames: complex storage one pair per frame, real two frames per pair.
+template <int S, int NF>
+struct FramePairs {
+    static constexpr int kValue = Storage<S>::kComplex ? NF : NF / 2;
+};
+
+// Widen 8 bytes of storage S into float2 pairs (same packing as the staged kernel's lanes).
+template <int S>
+__device__ __forceinline__ void widen8(uint2 r, float2* o);
+template <>
+__device__ __forceinline__ void widen8<kC64>(uint2 r, float2* o) {
+    o[0] = make_float2(__uint_as_float(r.x), __uint_as_float(r.y));
+}
+template <>
+__device__ __forceinline__ void widen8<kF32>(uint2 r, float2* o) {
+    o[0] = make_float2(__uint_as_float(r.x), __uint_as_float(r.y));
+}
+template <>
+__device__ __forceinline__ void widen8<kCF16>(uint2 r, float2* o) {
+    o[0] = __half22float2(*reinterpret_cast<const __half2*>(&r.x));
+    o[1] = __half22float2(*reinterpret_cast<const __half2*>(&r.y));
+}
+template <>
+__device__ __forceinline__ void widen8<kF16>(uint2 r, float2* o) {
+    widen8<kCF16>(r, o);
+}
+template <>
+__device__ __forceinline__ void widen8<kCBF16>(uint2 r, float2* o) {
+    o[0] = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&r.x));
+    o[1] = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&r.y));
+}
+template <>
+__device__ __forceinline__ void widen8<kBF16>(uint2 r, float2* o) {
+    widen8<kCBF16>(r, o);
+}
+// int16 pair of a 32-bit word -> exact floats without the conversion pipe: x + 32768 is
+// placed in the mantissa of 2^23 (bit pattern 0x4B000000 | u) and 2^23 + 32768 subtracted.
+__device__ __forceinline__ float2 widen_i16x2(unsigned w) {
+    const unsigned u = w ^ 0x80008000u;
+    const float lo = __uint_as_float(__byte_perm(u, 0x4B000000u, 0x7610));
+    const float hi = __uint_as_float(__byte_perm(u, 0x4B000000u, 0x7632));
+    return make_float2(__fsub_rn(lo, 8421376.0f), __fsub_rn(hi, 8421376.0f));
+}
+template <>
+__device__ __forceinline__ void widen8<kCI16>(uint2 r, float2* o) {
+    o[0] = widen_i16x2(r.x);
+    o[1] = widen_i16x2(r.y);
+}
+template <>
+__device__ __forceinline__ void widen8<kI16>(uint2 r, float2* o) {
+    widen8<kCI16>(r, o);
+}
+
+// Load the NF frames of one sample (NF * sizeof(T) is a multiple of 16 bytes).
+template <int S, int NF>
+__device__ __forceinline__ void load_frames(const typename Storage<S>::T* p, float2* o) {
+    constexpr int kBytes = NF * static_cast<int>(sizeof(typename Storage<S>::T));
+    static_assert(kBytes % 16 == 0, "vector frames need 16-byte rows");
+    constexpr int kPairsPer8 = FramePairs<S, NF>::kValue / (kBytes / 8);
+    const uint4* q = reinterpret_cast<const uint4*>(p);
+#pragma unroll
+    for (int i = 0; i < kBytes / 16; ++i) {
+        const uint4 r = __ldg(q + i);
+        widen8<S>(make_uint2(r.x, r.y), o + (2 * i) * kPairsPer8);
+        widen8<S>(make_uint2(r.z, r.w), o + (2 * i + 1) * kPairsPer8);
+    }
+}
+
 // Receive-path Tukey weight.  The weight only scales a sample, so fast intrinsics are used
 // (their ~1e-7 error is far inside the 1e-5 parity budget); the aperture decision itself is
 // the exact FP32 test of kernel.cu:461.
@@ -91,16 +196,22 @@ __device__ __forceinline__ float fast_tukey(float h2, float radius, const DasArg
     return __fmaf_rn(-0.5f, __cosf(__fdividef(kPi * (1.0f - r), a.alpha)), 0.5f);
 }
 
-template <int S, int INTERP, int NF>
-__global__ void __launch_bounds__(kLaneVoxelThreads, 8) das_lane_voxel_kernel(const __grid_constant__ DasArgs a) {
+// One CTA tile: voxels [tile * 128, tile * 128 + 128) of job `a`, all its transmits,
+// elements and frames.  `smem_words` is the dynamic shared memory (tx_chunk x 128 words,
+// x3 in split mode).  Shared by the per-job kernel and the persistent batch kernel.
+template <int S, int INTERP, int NF, bool SPLIT>
+__device__ __forceinline__ void lane_voxel_tile(const DasArgs& a, int64_t tile, float* smem_words) {
     using ST = Storage<S>;
     using T = typename ST::T;
     constexpr bool kCplx = ST::kComplex;
     constexpr unsigned kFull = 0xffffffffu;
-    extern __shared__ float s_arrival[];  // [tx_chunk][kLaneVoxelThreads]
+    // [tx_chunk][kLaneVoxelThreads] arrivals; split mode: sample base, fraction, phase cycles
+    float* const s_arrival = smem_words;
+    int* const s_base = reinterpret_cast<int*>(s_arrival + a.tx_chunk * kLaneVoxelThreads);
+    float* const s_cyc = s_arrival + 2 * a.tx_chunk * kLaneVoxelThreads;
 
     const int lane = threadIdx.x & 31;
-    const int64_t v = static_cast<int64_t>(blockIdx.x) * kLaneVoxelThreads + threadIdx.x;
+    const int64_t v = tile * kLaneVoxelThreads + threadIdx.x;
     const bool vox_ok = v < a.n_vox;
     const int n_frames = NF > 0 ? NF : a.n_frames;
 
@@ -126,7 +237,10 @@ __global__ void __launch_bounds__(kLaneVoxelThreads, 8) das_lane_voxel_kernel(co
     }
     const float cand_r2 = rmax * rmax * 1.00001f + 1e-30f;
 
-    constexpr int kAcc = NF > 0 ? NF : 8;
+    // Vector path: NF frames per sample loaded as 16-byte vectors, accumulated as float2
+    // pairs (complex: one frame per pair; real: two frames per pair).
+    constexpr bool kVec = NF >= 2 && (NF * static_cast<int>(sizeof(T))) % 16 == 0;
+    constexpr int kAcc = kVec ? FramePairs<S, NF>::kValue : (NF > 0 ? NF : 8);
     float2 acc[kAcc];
 #pragma unroll
     for (int f = 0; f < kAcc; ++f) acc[f] = make_float2(0.f, 0.f);
@@ -140,8 +254,17 @@ __global__ void __launch_bounds__(kLaneVoxelThreads, 8) das_lane_voxel_kernel(co
         __syncthreads();
         for (int i = threadIdx.x; i < nt * kLaneVoxelThreads; i += kLaneVoxelThreads) {
             const int t = i / kLaneVoxelThreads;
-            const int64_t vv = static_cast<int64_t>(blockIdx.x) * kLaneVoxelThreads + (i - t * kLaneVoxelThreads);
-            s_arrival[i] = vv < a.n_vox ? __ldg(a.arrivals + static_cast<int64_t>(t0 + t) * a.n_vox + vv) : 0.f;
+            const int64_t vv = tile * kLaneVoxelThreads + (i - t * kLaneVoxelThreads);
+            const float txa = vv < a.n_vox ? __ldg(a.arrivals + static_cast<int64_t>(t0 + t) * a.n_vox + vv) : 0.f;
+            if constexpr (SPLIT) {
+                // transmit part of the sample position and phase, per (voxel, transmit)
+                const SplitPos sp = split_position((static_cast<double>(txa) - a.t0_d) * a.fs_d);
+                s_base[i] = sp.base;
+                s_arrival[i] = sp.frac;
+                s_cyc[i] = reduced_cycles(static_cast<double>(txa) * a.fmod_d);
+            } else {
+                s_arrival[i] = txa;
+            }
         }
         __syncthreads();
 
@@ -163,11 +286,23 @@ __global__ void __launch_bounds__(kLaneVoxelThreads, 8) das_lane_voxel_kernel(co
                 cmask &= cmask - 1u;
 
                 // Receive path (kernel.cu:444-483), reused for every transmit below.
-                const float dx = __fsub_rn(__ldg(a.rx + 3 * e + 0), vx);
-                const float dy = __fsub_rn(__ldg(a.rx + 3 * e + 1), vy);
-                const float dz = __fsub_rn(__ldg(a.rx + 3 * e + 2), vz);
+                const float ex = __ldg(a.rx + 3 * e + 0), ey = __ldg(a.rx + 3 * e + 1), ez = __ldg(a.rx + 3 * e + 2);
+                const float dx = __fsub_rn(ex, vx);
+                const float dy = __fsub_rn(ey, vy);
+                const float dz = __fsub_rn(ez, vz);
                 const float h2 = __fmaf_rn(dx, dx, __fmul_rn(dy, dy));
-                const float dist = __fsqrt_rn(__fmaf_rn(dz, dz, h2));
+                float dist = 0.f;
+                SplitPos rx_pos{};
+                float rx_cyc = 0.f;
+                if constexpr (SPLIT) {
+                    const double ddx = static_cast<double>(ex) - vx, ddy = static_cast<double>(ey) - vy,
+                                 ddz = static_cast<double>(ez) - vz;
+                    const double d = sqrt(fma(ddx, ddx, fma(ddy, ddy, ddz * ddz)));
+                    rx_pos = split_position(d * a.fs_over_c);
+                    rx_cyc = reduced_cycles(d * a.fmod_over_c);
+                } else {
+                    dist = __fsqrt_rn(__fmaf_rn(dz, dz, h2));
+                }
                 float weight = 1.0f;
                 if (a.apod) weight = fast_tukey(h2, radius, a);
                 const bool pair_ok = vox_ok && !(h2 > radius_sq) && !(weight == 0.0f);
@@ -178,29 +313,85 @@ __global__ void __launch_bounds__(kLaneVoxelThreads, 8) das_lane_voxel_kernel(co
                 const int tx_step = a.n_rx * row_len;
 #pragma unroll 2
                 for (int t = 0; t < nt; ++t, row += tx_step) {
-                    const float tau = __fmaf_rn(dist, a.inv_c, s_arrival[t * kLaneVoxelThreads + threadIdx.x]);
-                    const float s = __fmul_rn(__fsub_rn(tau, a.t0), a.fs);
-                    bool ok = pair_ok && !(tau < 0.0f);
-                    if constexpr (INTERP == kNearest) {
-                        ok = ok && (s >= -0.5f) && (s <= a.hi_nearest);
-                    } else if constexpr (INTERP == kLinear) {
-                        ok = ok && (s >= 0.0f) && (s <= a.hi_linear);
-                    } else {
-                        ok = ok && (s >= 1.0f) && (s <= a.hi_quadratic);
-                    }
-                    if (!ok) continue;
-                    const TapPosition tp = tap_position<INTERP>(s);
-                    if constexpr (INTERP == kNearest) {
-                        if (tp.idx >= a.n_samples) continue;
-                    }
+                    const int si = t * kLaneVoxelThreads + threadIdx.x;
+                    TapPosition tp;
                     float cw = w, sw = 0.f;
-                    if (kCplx && a.rotate) {
-                        float sn, cs;
-                        __sincosf(__fmul_rn(a.mod_rad, tau), &sn, &cs);  // kernel.cu:656-658
-                        cw = __fmul_rn(cs, w);
-                        sw = __fmul_rn(sn, w);
+                    if constexpr (SPLIT) {
+                        // s = (tx part) + (receive part), as integer base + FP32 fraction
+                        int base = s_base[si] + rx_pos.base;
+                        float frac = __fadd_rn(s_arrival[si], rx_pos.frac);
+                        if (frac >= 1.0f) {
+                            frac = __fsub_rn(frac, 1.0f);
+                            base += 1;
+                        }
+                        // tau < 0  <=>  s < -t0 * fs
+                        bool ok = pair_ok && !(base < a.start_base || (base == a.start_base && frac < a.start_frac));
+                        ok = ok && split_tap_position<INTERP>(base, frac, a.n_samples, tp);
+                        if (!ok) continue;
+                        if (kCplx && a.rotate) {
+                            float sn, cs;
+                            split_phasor(__fadd_rn(s_cyc[si], rx_cyc), sn, cs);
+                            cw = __fmul_rn(cs, w);
+                            sw = __fmul_rn(sn, w);
+                        }
+                    } else {
+                        const float tau = __fmaf_rn(dist, a.inv_c, s_arrival[si]);
+                        const float s = __fmul_rn(__fsub_rn(tau, a.t0), a.fs);
+                        bool ok = pair_ok && !(tau < 0.0f);
+                        if constexpr (INTERP == kNearest) {
+                            ok = ok && (s >= -0.5f) && (s <= a.hi_nearest);
+                        } else if constexpr (INTERP == kLinear) {
+                            ok = ok && (s >= 0.0f) && (s <= a.hi_linear);
+                        } else {
+                            ok = ok && (s >= 1.0f) && (s <= a.hi_quadratic);
+                        }
+                        if (!ok) continue;
+                        tp = tap_position<INTERP>(s);
+                        if constexpr (INTERP == kNearest) {
+                            if (tp.idx >= a.n_samples) continue;
+                        }
+                        if (kCplx && a.rotate) {
+                            float sn, cs;
+                            __sincosf(__fmul_rn(a.mod_rad, tau), &sn, &cs);  // kernel.cu:656-658
+                            cw = __fmul_rn(cs, w);
+                            sw = __fmul_rn(sn, w);
+                        }
                     }
                     const T* p = channel + (row + tp.idx * n_frames);
+                    if constexpr (kVec) {
+                        float2 va[kAcc], vb[kAcc], vc[kAcc];
+                        if constexpr (INTERP == kNearest) {
+                            load_frames<S, NF>(p, va);
+                        } else if constexpr (INTERP == kLinear) {
+                            load_frames<S, NF>(p, va);
+                            load_frames<S, NF>(p + tp.step * NF, vb);
+                        } else {
+                            load_frames<S, NF>(p - NF, va);
+                            load_frames<S, NF>(p, vb);
+                            load_frames<S, NF>(p + NF, vc);
+                        }
+#pragma unroll
+                        for (int q = 0; q < kAcc; ++q) {
+                            float2 x;
+                            if constexpr (INTERP == kNearest) {
+                                x = va[q];
+                            } else if constexpr (INTERP == kLinear) {
+                                x.x = __fmaf_rn(tp.w0, __fsub_rn(vb[q].x, va[q].x), va[q].x);
+                                x.y = __fmaf_rn(tp.w0, __fsub_rn(vb[q].y, va[q].y), va[q].y);
+                            } else {
+                                x.x = __fmaf_rn(tp.w2, vc[q].x, __fmaf_rn(tp.w0, va[q].x, __fmul_rn(tp.w1, vb[q].x)));
+                                x.y = __fmaf_rn(tp.w2, vc[q].y, __fmaf_rn(tp.w0, va[q].y, __fmul_rn(tp.w1, vb[q].y)));
+                            }
+                            if constexpr (kCplx) {
+                                acc[q].x = __fmaf_rn(x.x, cw, __fmaf_rn(-x.y, sw, acc[q].x));
+                                acc[q].y = __fmaf_rn(x.y, cw, __fmaf_rn(x.x, sw, acc[q].y));
+                            } else {
+                                acc[q].x = __fmaf_rn(x.x, cw, acc[q].x);
+                                acc[q].y = __fmaf_rn(x.y, cw, acc[q].y);
+                            }
+                        }
+                        continue;
+                    }
 #pragma unroll
                     for (int f = 0; f < kAcc; ++f) {
                         if (NF > 0 || f < n_frames) {
@@ -219,6 +410,26 @@ __global__ void __launch_bounds__(kLaneVoxelThreads, 8) das_lane_voxel_kernel(co
     }
 
     if (!vox_ok) return;
+    if constexpr (kVec) {
+#pragma unroll
+        for (int q = 0; q < kAcc; ++q) {
+            if constexpr (kCplx) {
+                float2* out = static_cast<float2*>(a.out) + v * NF + q;
+                float2 r = acc[q];
+                if (a.accumulate) {
+                    const float2 prev = *out;
+                    r.x = __fadd_rn(prev.x, r.x);
+                    r.y = __fadd_rn(prev.y, r.y);
+                }
+                *out = r;
+            } else {
+                float* out = static_cast<float*>(a.out) + v * NF + 2 * q;
+                out[0] = a.accumulate ? __fadd_rn(out[0], acc[q].x) : acc[q].x;
+                out[1] = a.accumulate ? __fadd_rn(out[1], acc[q].y) : acc[q].y;
+            }
+        }
+        return;
+    }
 #pragma unroll
     for (int f = 0; f < kAcc; ++f) {
         if (NF > 0 || f < n_frames) {
@@ -238,6 +449,115 @@ __global__ void __launch_bounds__(kLaneVoxelThreads, 8) das_lane_voxel_kernel(co
             }
         }
     }
+}
+
+// ---- per-point parameters shared by the warp-per-voxel kernel ----
+
+// Receive path of one (voxel, element) pair in either delay mode.
+struct PairRx {
+    float dist;    // reference mode: FP32 distance (kernel.cu:467)
+    SplitPos pos;  // split mode: receive part of the sample position
+    float cyc;     // split mode: receive part of the phase (cycles)
+    float w;       // apodisation weight x storage scale
+};
+
+__device__ __forceinline__ bool pair_receive(const DasArgs& a, float ex, float ey, float ez, float vx, float vy,
+                                             float vz, float radius, float radius_sq, PairRx& rx) {
+    const float dx = __fsub_rn(ex, vx);
+    const float dy = __fsub_rn(ey, vy);
+    const float dz = __fsub_rn(ez, vz);
+    const float h2 = __fmaf_rn(dx, dx, __fmul_rn(dy, dy));
+    if (a.split) {
+        const double ddx = static_cast<double>(ex) - vx, ddy = static_cast<double>(ey) - vy,
+                     ddz = static_cast<double>(ez) - vz;
+        const double d = sqrt(fma(ddx, ddx, fma(ddy, ddy, ddz * ddz)));
+        rx.pos = split_position(d * a.fs_over_c);
+        rx.cyc = reduced_cycles(d * a.fmod_over_c);
+    } else {
+        rx.dist = __fsqrt_rn(__fmaf_rn(dz, dz, h2));
+    }
+    float weight = 1.0f;
+    if (a.apod) weight = fast_tukey(h2, radius, a);
+    rx.w = __fmul_rn(weight, a.scale);
+    return !(h2 > radius_sq) && !(weight == 0.0f);  // kernel.cu:461, 634
+}
+
+// Transmit part of one point: tap index, interpolation parameter (linear: t, quadratic: x
+// from the centre tap) and the weighted phasor.  Returns false when the point is skipped.
+template <int INTERP, bool CPLX>
+__device__ __forceinline__ bool point_taps(const DasArgs& a, const PairRx& rx, float txa, int& idx, float& w,
+                                           float& cw, float& sw) {
+    TapPosition tp{};
+    float sn = 0.f, cs = 1.f;
+    bool ok;
+    if (a.split) {
+        const SplitPos tx = split_position((static_cast<double>(txa) - a.t0_d) * a.fs_d);
+        int base = tx.base + rx.pos.base;
+        float frac = __fadd_rn(tx.frac, rx.pos.frac);
+        if (frac >= 1.0f) {
+            frac = __fsub_rn(frac, 1.0f);
+            base += 1;
+        }
+        ok = !(base < a.start_base || (base == a.start_base && frac < a.start_frac));
+        ok = ok && split_tap_position<INTERP>(base, frac, a.n_samples, tp);
+        if (ok) w = INTERP == kQuadratic ? __fsub_rn(frac, static_cast<float>(tp.idx - base)) : tp.w0;
+        if (ok && CPLX && a.rotate) split_phasor(__fadd_rn(reduced_cycles(static_cast<double>(txa) * a.fmod_d), rx.cyc), sn, cs);
+    } else {
+        const float tau = __fmaf_rn(rx.dist, a.inv_c, txa);
+        const float s = __fmul_rn(__fsub_rn(tau, a.t0), a.fs);
+        ok = !(tau < 0.0f);
+        if constexpr (INTERP == kNearest) {
+            ok = ok && (s >= -0.5f) && (s <= a.hi_nearest);
+        } else if constexpr (INTERP == kLinear) {
+            ok = ok && (s >= 0.0f) && (s <= a.hi_linear);
+        } else {
+            ok = ok && (s >= 1.0f) && (s <= a.hi_quadratic);
+        }
+        tp = tap_position<INTERP>(s);
+        if constexpr (INTERP == kNearest) ok = ok && tp.idx < a.n_samples;
+        if (ok) w = INTERP == kQuadratic ? __fsub_rn(s, static_cast<float>(tp.idx)) : tp.w0;
+        if (ok && CPLX && a.rotate) __sincosf(__fmul_rn(a.mod_rad, tau), &sn, &cs);  // kernel.cu:656-658
+    }
+    idx = tp.idx;
+    cw = rx.w;
+    sw = 0.f;
+    if (ok && CPLX && a.rotate) {
+        cw = __fmul_rn(cs, rx.w);
+        sw = __fmul_rn(sn, rx.w);
+    }
+    return ok;
+}
+
+// Interpolated sample from tap index `idx` and parameter `w` (see point_taps); `row`
+// already points at the frame, samples are `stride` apart.
+template <int S, int INTERP>
+__device__ __forceinline__ float2 gather_taps(const typename Storage<S>::T* row, int idx, float w, int64_t stride) {
+    using ST = Storage<S>;
+    const typename ST::T* p = row + static_cast<int64_t>(idx) * stride;
+    if constexpr (INTERP == kNearest) {
+        return ST::load(p);
+    } else if constexpr (INTERP == kLinear) {
+        const float2 lo = ST::load(p);
+        const float2 hi = ST::load(p + (w > 0.0f ? stride : 0));
+        return make_float2(__fmaf_rn(w, __fsub_rn(hi.x, lo.x), lo.x),
+                           ST::kComplex ? __fmaf_rn(w, __fsub_rn(hi.y, lo.y), lo.y) : 0.f);
+    } else {
+        const float hx = __fmul_rn(0.5f, w);
+        const float q = __fmul_rn(hx, w);
+        const float wm = __fsub_rn(q, hx), w0 = __fmaf_rn(-2.0f, q, 1.0f), wp = __fadd_rn(q, hx);
+        const float2 dm = ST::load(p - stride);
+        const float2 d0 = ST::load(p);
+        const float2 dp = ST::load(p + stride);
+        return make_float2(__fmaf_rn(wp, dp.x, __fmaf_rn(wm, dm.x, __fmul_rn(w0, d0.x))),
+                           ST::kComplex ? __fmaf_rn(wp, dp.y, __fmaf_rn(wm, dm.y, __fmul_rn(w0, d0.y))) : 0.f);
+    }
+}
+
+template <int S, int INTERP, int NF, bool SPLIT>
+__global__ void __launch_bounds__(kLaneVoxelThreads, NF == 16 ? 4 : 8)
+    das_lane_voxel_kernel(const __grid_constant__ DasArgs a) {
+    extern __shared__ float smem_words[];
+    lane_voxel_tile<S, INTERP, NF, SPLIT>(a, blockIdx.x, smem_words);
 }
 
 }  // namespace mach_b200

@@ -1,6 +1,10 @@
 // Kernel selection and launch for one storage type.
 #pragma once
 
+#include <algorithm>
+
+#include "das_batch.cuh"
+#include "das_ensemble.cuh"
 #include "das_gather.cuh"
 #include "das_lane_voxel.cuh"
 #include "das_staged.cuh"
@@ -13,6 +17,8 @@ enum KernelKind : int {
     kKindWarpHalf = 2,     // das_gather_kernel, 16 lanes per voxel
     kKindWarp = 3,         // das_gather_kernel, 32 lanes per voxel
     kKindStaged = 4,       // das_staged_kernel, windows staged in shared memory (TMA or direct)
+    kKindLaneVoxel16 = 5,  // das_lane_voxel_kernel, exactly 16 frames loaded as 16-byte vectors
+    kKindEnsemble = 6,     // das_ensemble_kernel, windows in tensor memory, lanes = frames
 };
 
 struct LaunchPlan {
@@ -42,6 +48,13 @@ cudaError_t launch_staged(const DasArgs& a, const StagedArgs& st, const CUtensor
     return cudaGetLastError();
 }
 
+// Storage types with two float2 pairs per 8-byte lane vector stop at 16 lanes per voxel
+// (32 would need 64 accumulator registers per thread); the planner never asks for more.
+template <int S>
+constexpr int max_lanes_per_voxel() {
+    return Vec8<S>::kPairs == 2 ? 16 : 32;
+}
+
 template <int S, int I>
 cudaError_t launch_staged_lv(const DasArgs& a, const StagedArgs& st, const CUtensorMap& map, const LaunchPlan& p,
                              cudaStream_t stream) {
@@ -49,7 +62,7 @@ cudaError_t launch_staged_lv(const DasArgs& a, const StagedArgs& st, const CUten
         case 4: return launch_staged<S, I, 4>(a, st, map, p, stream);
         case 8: return launch_staged<S, I, 8>(a, st, map, p, stream);
         case 16: return launch_staged<S, I, 16>(a, st, map, p, stream);
-        default: return launch_staged<S, I, 32>(a, st, map, p, stream);
+        default: return launch_staged<S, I, max_lanes_per_voxel<S>()>(a, st, map, p, stream);
     }
 }
 
@@ -65,12 +78,17 @@ cudaError_t launch_das_staged(const DasArgs& a, const StagedArgs& st, const CUte
 
 template <int S>
 cudaError_t launch_das(const DasArgs& a, int interp, const LaunchPlan& p, cudaStream_t stream) {
-#define MACH_B200_LV(I, NF) das_lane_voxel_kernel<S, I, NF><<<p.grid, p.block, p.smem, stream>>>(a)
+#define MACH_B200_LV(I, NF)                                                                   \
+    do {                                                                                      \
+        if (a.split) das_lane_voxel_kernel<S, I, NF, true><<<p.grid, p.block, p.smem, stream>>>(a);  \
+        else das_lane_voxel_kernel<S, I, NF, false><<<p.grid, p.block, p.smem, stream>>>(a);         \
+    } while (0)
 #define MACH_B200_WG(I, L, P) das_gather_kernel<S, I, L, P><<<p.grid, p.block, 0, stream>>>(a)
 #define MACH_B200_KINDS(I)                                   \
     switch (p.kind) {                                        \
         case kKindLaneVoxel1: MACH_B200_LV(I, 1); break;     \
         case kKindLaneVoxelN: MACH_B200_LV(I, 0); break;     \
+        case kKindLaneVoxel16: MACH_B200_LV(I, 16); break;   \
         case kKindWarpHalf: MACH_B200_WG(I, 16, 4); break;   \
         default: MACH_B200_WG(I, 32, 8); break;              \
     }
@@ -83,6 +101,100 @@ cudaError_t launch_das(const DasArgs& a, int interp, const LaunchPlan& p, cudaSt
 #undef MACH_B200_WG
 #undef MACH_B200_LV
     return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------- persistent batch launches
+
+struct PersistentLaunch {
+    const BatchHeader* hdr;
+    const BatchJob* jobs;
+    const int64_t* item_begin;
+    unsigned long long* counter;
+    size_t smem;
+    int max_items;  // grid is min(max_items, resident CTAs)
+};
+
+template <typename K>
+cudaError_t launch_persistent(K kernel, int threads, const PersistentLaunch& pl, cudaStream_t stream) {
+    cudaError_t e = allow_smem(kernel, pl.smem);
+    if (e != cudaSuccess) return e;
+    int device = 0, sms = 0, per_sm = 0;
+    if ((e = cudaGetDevice(&device)) != cudaSuccess) return e;
+    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device)) != cudaSuccess) return e;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, pl.smem)) != cudaSuccess) return e;
+    const int grid = std::max(1, std::min(pl.max_items, std::max(1, per_sm) * sms));
+    kernel<<<grid, threads, pl.smem, stream>>>(pl.hdr, pl.jobs, pl.item_begin, pl.counter);
+    return cudaGetLastError();
+}
+
+// Lane-voxel family: frame class 1 (one frame), 0 (2..8 frames), 16 (sixteen, vectorised).
+template <int S>
+cudaError_t launch_lane_voxel_persistent(int interp, int frame_class, bool split, const PersistentLaunch& pl,
+                                         cudaStream_t stream) {
+#define MACH_B200_PLV(I, NF)                                                                              \
+    return split ? launch_persistent(das_lane_voxel_persistent<S, I, NF, true>, kLaneVoxelThreads, pl, stream) \
+                 : launch_persistent(das_lane_voxel_persistent<S, I, NF, false>, kLaneVoxelThreads, pl, stream)
+#define MACH_B200_PLV_NF(I)                         \
+    switch (frame_class) {                          \
+        case 1: MACH_B200_PLV(I, 1);                \
+        case 16: MACH_B200_PLV(I, 16);              \
+        default: MACH_B200_PLV(I, 0);               \
+    }
+    switch (interp) {
+        case kNearest: MACH_B200_PLV_NF(kNearest)
+        case kLinear: MACH_B200_PLV_NF(kLinear)
+        default: MACH_B200_PLV_NF(kQuadratic)
+    }
+#undef MACH_B200_PLV_NF
+#undef MACH_B200_PLV
+}
+
+template <int S>
+cudaError_t launch_staged_persistent(int interp, int lanes, const PersistentLaunch& pl, cudaStream_t stream) {
+#define MACH_B200_PST(I, LV) return launch_persistent(das_staged_persistent<S, I, LV>, kStagedThreads, pl, stream)
+#define MACH_B200_PST_LV(I)                                    \
+    switch (lanes) {                                           \
+        case 4: MACH_B200_PST(I, 4);                           \
+        case 8: MACH_B200_PST(I, 8);                           \
+        case 16: MACH_B200_PST(I, 16);                         \
+        default: MACH_B200_PST(I, max_lanes_per_voxel<S>());   \
+    }
+    switch (interp) {
+        case kNearest: MACH_B200_PST_LV(kNearest)
+        case kLinear: MACH_B200_PST_LV(kLinear)
+        default: MACH_B200_PST_LV(kQuadratic)
+    }
+#undef MACH_B200_PST_LV
+#undef MACH_B200_PST
+}
+
+// Ensemble kernel: persistent grid of at most one CTA per SM (its 512 threads use the whole
+// register file), each CTA running four teams over the (tile, frame block) items.
+template <int S, int I, bool SPLIT>
+cudaError_t launch_ensemble(const DasArgs& a, const StagedArgs& st, const EnsembleArgs& ea, const CUtensorMap& map,
+                            size_t smem, cudaStream_t stream) {
+    auto kernel = das_ensemble_kernel<S, I, SPLIT>;
+    cudaError_t e = allow_smem(kernel, smem);
+    if (e != cudaSuccess) return e;
+    int device = 0, sms = 0, per_sm = 0;
+    if ((e = cudaGetDevice(&device)) != cudaSuccess) return e;
+    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device)) != cudaSuccess) return e;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kEnsThreads, smem)) != cudaSuccess) return e;
+    const int items = ea.n_tiles * ea.n_fblocks;
+    const int grid = std::max(1, std::min((items + kEnsTeams - 1) / kEnsTeams, std::max(1, per_sm) * sms));
+    kernel<<<grid, kEnsThreads, smem, stream>>>(a, st, ea, map);
+    return cudaGetLastError();
+}
+
+template <int S>
+cudaError_t launch_das_ensemble(const DasArgs& a, const StagedArgs& st, const EnsembleArgs& ea, const CUtensorMap& map,
+                                int interp, size_t smem, cudaStream_t stream) {
+    if (interp == kNearest) {
+        return a.split ? launch_ensemble<S, kNearest, true>(a, st, ea, map, smem, stream)
+                       : launch_ensemble<S, kNearest, false>(a, st, ea, map, smem, stream);
+    }
+    return a.split ? launch_ensemble<S, kLinear, true>(a, st, ea, map, smem, stream)
+                   : launch_ensemble<S, kLinear, false>(a, st, ea, map, smem, stream);
 }
 
 }  // namespace mach_b200

@@ -139,6 +139,9 @@ __device__ __forceinline__ uint32_t smem_addr(const void* p) {
 __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
 }
+__device__ __forceinline__ void mbar_inval(uint64_t* bar) {
+    asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
 __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
                  : "memory");
@@ -187,19 +190,22 @@ __device__ __forceinline__ int64_t tile_voxel(const DasArgs& a, const StagedArgs
     return (static_cast<int64_t>(s) * st.grid_mid + m) * st.grid_fast + f;
 }
 
-// Per-voxel step parameters in shared memory (8 words).
+// Per-voxel step parameters in shared memory (16 bytes, one broadcast load per round).
 struct StepParam {
-    int row;    // tap centre row (TMA: relative to the window; direct: absolute in the element row); -1 = skip
-    float w0, w1, w2;
-    float cw, sw;
-    int step;   // linear: 1 when the second tap differs
-    int pad;
+    int row;   // tap row (TMA mode: absolute sample index, the window start is subtracted later)
+    float w;   // linear: fraction t; quadratic: offset x from the centre tap; nearest: unused
+    float cw;  // weight x cos(phase) (real data: the weight)
+    float sw;  // weight x sin(phase)
 };
 
+constexpr int kMaxPrefetchTx = 32;  // transmit arrivals of the tile staged once in shared memory
+
+// One CTA tile: the tile's 128 voxels x frame chunk `chunk` of job `a`.  `tmap` must live in
+// parameter, constant or global memory.  Shared by the per-job and persistent kernels.
 template <int S, int INTERP, int LV>
-__global__ void __launch_bounds__(kStagedThreads, 1)
-    das_staged_kernel(const __grid_constant__ DasArgs a, const __grid_constant__ StagedArgs st,
-                      const __grid_constant__ CUtensorMap tmap) {
+// Returns false if a wait timed out (the caller must then stop using this CTA).
+__device__ __forceinline__ bool staged_tile(const DasArgs& a, const StagedArgs& st, const CUtensorMap* tmap,
+                                            int tile, int chunk, unsigned char* smem) {
     using ST = Storage<S>;
     using T = typename ST::T;
     constexpr bool kCplx = ST::kComplex;
@@ -209,20 +215,24 @@ __global__ void __launch_bounds__(kStagedThreads, 1)
     constexpr int G = 32 / LV;                  // voxel streams per warp
     constexpr int ROUNDS = kVoxelsPerWarp / G;  // voxels per stream
     constexpr int FC = LV * VF;                 // frames per CTA
+    constexpr int kRowBytes = FC * kEsz;        // one window row
     constexpr unsigned kFull = 0xffffffffu;
+    constexpr unsigned kGroupMask = (1u << G) - 1u;
     static_assert(kVoxelsPerWarp % G == 0, "lane shape");
 
-    extern __shared__ __align__(128) unsigned char smem[];
     const int W = st.window_rows;
-    const int window_bytes = W * FC * kEsz;
-    unsigned char* s_window = smem;                                   // [2][W][FC] of T
+    const int window_bytes = W * kRowBytes;
+    unsigned char* s_window = smem;                                                // [2][W][FC] of T
     StepParam* s_param = reinterpret_cast<StepParam*>(smem + 2 * window_bytes);  // [3][128]
-    int* s_cand = reinterpret_cast<int*>(s_param + 3 * kTileVoxels);  // [kMaxElemBlock]
-    int* s_lohi = s_cand + kMaxElemBlock;                             // [3][kStagedWarps][2] partial windows
-    int* s_lo = s_lohi + 3 * kStagedWarps * 2;                        // [3] window start per step
-    int* s_mode = s_lo + 3;                                           // [3] 0 empty, 1 TMA, 2 direct
-    int* s_count = s_mode + 3;                                        // [kStagedWarps + 1] compaction
-    float* s_bbox = reinterpret_cast<float*>(s_count + kStagedWarps + 1);  // [kStagedWarps][5]
+    float* s_arr = reinterpret_cast<float*>(s_param + 3 * kTileVoxels);           // [n_pref][128]
+    const int n_pref = a.n_tx <= kMaxPrefetchTx ? a.n_tx : 0;
+    int* s_cand = reinterpret_cast<int*>(s_arr + n_pref * kTileVoxels);           // [kMaxElemBlock]
+    int* s_lohi = s_cand + kMaxElemBlock;  // [3][4][2] per-parameter-warp window partials
+    unsigned* s_valid = reinterpret_cast<unsigned*>(s_lohi + 3 * 4 * 2);  // [3][4] validity ballots
+    int* s_lo = reinterpret_cast<int*>(s_valid + 3 * 4);                 // [3] window start per step
+    int* s_mode = s_lo + 3;                                               // [3] 0 empty, 1 TMA, 2 direct
+    int* s_count = s_mode + 3;                                            // [kStagedWarps] compaction
+    float* s_bbox = reinterpret_cast<float*>(s_count + kStagedWarps);     // [kStagedWarps][5]
     uint64_t* s_bar = reinterpret_cast<uint64_t*>(
         (reinterpret_cast<uintptr_t>(s_bbox + kStagedWarps * 5) + 7) & ~uintptr_t{7});  // [2]
 
@@ -231,15 +241,15 @@ __global__ void __launch_bounds__(kStagedThreads, 1)
     const int warp = tid >> 5;
     const int g = lane / LV;
     const int sub = lane - g * LV;
-    const int frame0 = static_cast<int>(blockIdx.y) * FC + sub * VF;
+    const int frame0 = chunk * FC + sub * VF;
     const bool frames_ok = frame0 < a.n_frames;
     const T* const channel = static_cast<const T*>(a.channel);
     const int64_t n_frames = a.n_frames;
     const int64_t row_len = static_cast<int64_t>(a.n_samples);
 
-    // ---- the parameter thread's voxel
+    // ---- the parameter thread's voxel (threads 0..127)
     const bool is_param = tid < kTileVoxels;
-    const int64_t pv = is_param ? tile_voxel(a, st, blockIdx.x, tid) : -1;
+    const int64_t pv = is_param ? tile_voxel(a, st, tile, tid) : -1;
     float vx = 0.f, vy = 0.f, vz = 0.f;
     if (pv >= 0) {
         vx = __ldg(a.scan + 3 * pv + 0);
@@ -249,7 +259,12 @@ __global__ void __launch_bounds__(kStagedThreads, 1)
     const float radius = __fdiv_rn(vz, a.two_f_number);  // kernel.cu:583
     const float radius_sq = __fmul_rn(radius, radius);
 
-    // ---- tile bounding box for the candidate-element test
+    // ---- stage the tile's transmit arrivals; tile bounding box for the candidate test
+    for (int i = tid; i < n_pref * kTileVoxels; i += kStagedThreads) {
+        const int t = i / kTileVoxels;
+        const int64_t vv = tile_voxel(a, st, tile, i - t * kTileVoxels);
+        s_arr[i] = vv >= 0 ? __ldg(a.arrivals + static_cast<int64_t>(t) * a.n_vox + vv) : 0.f;
+    }
     {
         float b[5] = {pv >= 0 ? vx : INFINITY, pv >= 0 ? -vx : INFINITY, pv >= 0 ? vy : INFINITY,
                       pv >= 0 ? -vy : INFINITY, pv >= 0 ? -fabsf(radius) : INFINITY};
@@ -293,6 +308,8 @@ __global__ void __launch_bounds__(kStagedThreads, 1)
     int rx_elem = -1;
     float dist = 0.f, weight_scaled = 0.f;
     bool pair_ok = false;
+    SplitPos rx_pos{};
+    float rx_cyc = 0.f;
 
     for (int eb = 0; eb < a.n_rx; eb += kMaxElemBlock) {
         // ---- candidate elements of this block (compacted, in element order)
@@ -306,7 +323,7 @@ __global__ void __launch_bounds__(kStagedThreads, 1)
             cand = ddx * ddx + ddy * ddy <= cand_r2;
         }
         const unsigned m = __ballot_sync(kFull, cand);
-        __syncthreads();  // previous block's s_cand / s_count fully consumed
+        __syncthreads();  // the previous block's s_cand is fully consumed
         if (lane == 0) s_count[warp] = __popc(m);
         __syncthreads();
         int base = 0, total = 0;
@@ -321,33 +338,60 @@ __global__ void __launch_bounds__(kStagedThreads, 1)
         if (total == 0) continue;
         const int n_steps = total * a.n_tx;
 
-        // ---- parameters of step k into slot k % 3 (parameter threads), window partials
+        // ---- parameters of step k into slot k % 3 (parameter threads), window partials, ballots
         auto make_params = [&](int k) {
+            if (!is_param) return;
             const int ci = k / a.n_tx;
             const int t = k - ci * a.n_tx;
             const int e = s_cand[ci];
             const int slot = k % 3;
-            if (is_param) {
-                if (e != rx_elem) {
-                    rx_elem = e;
-                    const float dx = __fsub_rn(__ldg(a.rx + 3 * e + 0), vx);
-                    const float dy = __fsub_rn(__ldg(a.rx + 3 * e + 1), vy);
-                    const float dz = __fsub_rn(__ldg(a.rx + 3 * e + 2), vz);
-                    const float h2 = __fmaf_rn(dx, dx, __fmul_rn(dy, dy));
+            if (e != rx_elem) {
+                rx_elem = e;
+                const float ex = __ldg(a.rx + 3 * e + 0), ey = __ldg(a.rx + 3 * e + 1), ez = __ldg(a.rx + 3 * e + 2);
+                const float dx = __fsub_rn(ex, vx);
+                const float dy = __fsub_rn(ey, vy);
+                const float dz = __fsub_rn(ez, vz);
+                const float h2 = __fmaf_rn(dx, dx, __fmul_rn(dy, dy));
+                if (a.split) {
+                    const double ddx = static_cast<double>(ex) - vx, ddy = static_cast<double>(ey) - vy,
+                                 ddz = static_cast<double>(ez) - vz;
+                    const double d = sqrt(fma(ddx, ddx, fma(ddy, ddy, ddz * ddz)));
+                    rx_pos = split_position(d * a.fs_over_c);
+                    rx_cyc = reduced_cycles(d * a.fmod_over_c);
+                } else {
                     dist = __fsqrt_rn(__fmaf_rn(dz, dz, h2));  // kernel.cu:467
-                    float weight = 1.0f;
-                    if (a.apod) weight = fast_tukey(h2, radius, a);
-                    pair_ok = pv >= 0 && !(h2 > radius_sq) && !(weight == 0.0f);
-                    weight_scaled = __fmul_rn(weight, a.scale);
                 }
-                StepParam p{};
-                p.row = -1;
-                int lo = 0x7fffffff, hi = -1;
-                if (pair_ok) {
-                    const float tau =
-                        __fmaf_rn(dist, a.inv_c, __ldg(a.arrivals + static_cast<int64_t>(t) * a.n_vox + pv));
+                float weight = 1.0f;
+                if (a.apod) weight = fast_tukey(h2, radius, a);
+                pair_ok = pv >= 0 && !(h2 > radius_sq) && !(weight == 0.0f);
+                weight_scaled = __fmul_rn(weight, a.scale);
+            }
+            StepParam p{-1, 0.f, 0.f, 0.f};
+            int lo = 0x7fffffff, hi = -1;
+            bool ok = false;
+            if (pair_ok) {
+                const float txa = n_pref ? s_arr[t * kTileVoxels + tid]
+                                         : __ldg(a.arrivals + static_cast<int64_t>(t) * a.n_vox + pv);
+                TapPosition tp{};
+                float sn = 0.f, cs = 1.f;
+                if (a.split) {
+                    const SplitPos tx_pos = split_position((static_cast<double>(txa) - a.t0_d) * a.fs_d);
+                    int sbase = tx_pos.base + rx_pos.base;
+                    float frac = __fadd_rn(tx_pos.frac, rx_pos.frac);
+                    if (frac >= 1.0f) {
+                        frac = __fsub_rn(frac, 1.0f);
+                        sbase += 1;
+                    }
+                    ok = !(sbase < a.start_base || (sbase == a.start_base && frac < a.start_frac));
+                    ok = ok && split_tap_position<INTERP>(sbase, frac, a.n_samples, tp);
+                    if (INTERP == kQuadratic && ok) tp.w0 = __fsub_rn(frac, static_cast<float>(tp.idx - sbase));
+                    if (ok && kCplx && a.rotate) {
+                        split_phasor(__fadd_rn(reduced_cycles(static_cast<double>(txa) * a.fmod_d), rx_cyc), sn, cs);
+                    }
+                } else {
+                    const float tau = __fmaf_rn(dist, a.inv_c, txa);
                     const float s = __fmul_rn(__fsub_rn(tau, a.t0), a.fs);
-                    bool ok = !(tau < 0.0f);
+                    ok = !(tau < 0.0f);
                     if constexpr (INTERP == kNearest) {
                         ok = ok && (s >= -0.5f) && (s <= a.hi_nearest);
                     } else if constexpr (INTERP == kLinear) {
@@ -355,36 +399,36 @@ __global__ void __launch_bounds__(kStagedThreads, 1)
                     } else {
                         ok = ok && (s >= 1.0f) && (s <= a.hi_quadratic);
                     }
-                    const TapPosition tp = tap_position<INTERP>(s);
+                    tp = tap_position<INTERP>(s);
                     if constexpr (INTERP == kNearest) ok = ok && tp.idx < a.n_samples;
-                    if (ok) {
-                        p.row = tp.idx;
-                        p.w0 = tp.w0;
-                        p.w1 = tp.w1;
-                        p.w2 = tp.w2;
-                        p.step = tp.step;
-                        p.cw = weight_scaled;
-                        p.sw = 0.f;
-                        if (kCplx && a.rotate) {
-                            float sn, cs;
-                            __sincosf(__fmul_rn(a.mod_rad, tau), &sn, &cs);  // kernel.cu:656-658
-                            p.cw = __fmul_rn(cs, weight_scaled);
-                            p.sw = __fmul_rn(sn, weight_scaled);
-                        }
-                        lo = INTERP == kQuadratic ? tp.idx - 1 : tp.idx;
-                        hi = INTERP == kQuadratic ? tp.idx + 1 : (INTERP == kLinear ? tp.idx + tp.step : tp.idx);
+                    if constexpr (INTERP == kQuadratic) tp.w0 = __fsub_rn(s, static_cast<float>(tp.idx));
+                    if (ok && kCplx && a.rotate) {
+                        __sincosf(__fmul_rn(a.mod_rad, tau), &sn, &cs);  // kernel.cu:656-658
                     }
                 }
-                s_param[slot * kTileVoxels + tid] = p;
+                if (ok) {
+                    p.row = tp.idx;
+                    p.w = tp.w0;  // linear: t; quadratic: x (weights rebuilt in the gather)
+                    p.cw = weight_scaled;
+                    if (kCplx && a.rotate) {
+                        p.cw = __fmul_rn(cs, weight_scaled);
+                        p.sw = __fmul_rn(sn, weight_scaled);
+                    }
+                    lo = INTERP == kQuadratic ? tp.idx - 1 : tp.idx;
+                    hi = INTERP == kQuadratic ? tp.idx + 1 : (INTERP == kLinear ? tp.idx + tp.step : tp.idx);
+                }
+            }
+            s_param[slot * kTileVoxels + tid] = p;
+            const unsigned vmask = __ballot_sync(kFull, ok);
 #pragma unroll
-                for (int off = 16; off > 0; off >>= 1) {
-                    lo = min(lo, __shfl_xor_sync(kFull, lo, off));
-                    hi = max(hi, __shfl_xor_sync(kFull, hi, off));
-                }
-                if (lane == 0) {
-                    s_lohi[(slot * kStagedWarps + warp) * 2 + 0] = lo;
-                    s_lohi[(slot * kStagedWarps + warp) * 2 + 1] = hi;
-                }
+            for (int off = 16; off > 0; off >>= 1) {
+                lo = min(lo, __shfl_xor_sync(kFull, lo, off));
+                hi = max(hi, __shfl_xor_sync(kFull, hi, off));
+            }
+            if (lane == 0) {
+                s_lohi[(slot * 4 + warp) * 2 + 0] = lo;
+                s_lohi[(slot * 4 + warp) * 2 + 1] = hi;
+                s_valid[slot * 4 + warp] = vmask;
             }
         };
         // ---- after the barrier: decide how step k reads its taps, and start its window copy
@@ -392,9 +436,10 @@ __global__ void __launch_bounds__(kStagedThreads, 1)
             if (tid != 0) return;
             const int slot = k % 3;
             int lo = 0x7fffffff, hi = -1;
-            for (int w = 0; w < kTileVoxels / 32; ++w) {
-                lo = min(lo, s_lohi[(slot * kStagedWarps + w) * 2 + 0]);
-                hi = max(hi, s_lohi[(slot * kStagedWarps + w) * 2 + 1]);
+#pragma unroll
+            for (int w = 0; w < 4; ++w) {
+                lo = min(lo, s_lohi[(slot * 4 + w) * 2 + 0]);
+                hi = max(hi, s_lohi[(slot * 4 + w) * 2 + 1]);
             }
             int mode = 0;
             if (hi >= lo) mode = (st.use_tma && hi - lo + 1 <= W) ? 1 : 2;
@@ -407,7 +452,7 @@ __global__ void __launch_bounds__(kStagedThreads, 1)
                 const int b = k & 1;
                 const int row0 = (t * a.n_rx + e) * a.n_samples + lo;
                 mbar_expect_tx(&s_bar[b], static_cast<uint32_t>(window_bytes));
-                tma_load_2d(s_window + b * window_bytes, &tmap, static_cast<int>(blockIdx.y) * FC, row0, &s_bar[b]);
+                tma_load_2d(s_window + b * window_bytes, tmap, chunk * FC, row0, &s_bar[b]);
             }
         };
 
@@ -429,39 +474,42 @@ __global__ void __launch_bounds__(kStagedThreads, 1)
                 if (!timed_out && !mbar_wait(&s_bar[b], phase[b])) timed_out = true;
                 phase[b] ^= 1u;
             }
-            if (timed_out) continue;
+            if (timed_out || !frames_ok) continue;
+            // This warp's 16 voxels are bits [16 (warp & 1), +16) of parameter warp warp / 2.
+            const unsigned wmask = (s_valid[slot * 4 + (warp >> 1)] >> ((warp & 1) * 16)) & 0xffffu;
+            if (wmask == 0u) continue;
             const int ci = k / a.n_tx;
             const int t = k - ci * a.n_tx;
             const int e = s_cand[ci];
             const int lo = s_lo[slot];
-            // Tap addressing: TMA window rows are FC frames apart; global rows n_frames apart.
-            const unsigned char* win = s_window + b * window_bytes;
-            const T* grow = channel + static_cast<int64_t>(t * a.n_rx + e) * row_len * n_frames;
+            const unsigned char* win = s_window + b * window_bytes + sub * VF * kEsz;
+            const T* grow = channel + static_cast<int64_t>(t * a.n_rx + e) * row_len * n_frames + frame0;
+            const StepParam* prm = s_param + slot * kTileVoxels + warp * kVoxelsPerWarp + g;
 #pragma unroll
             for (int r = 0; r < ROUNDS; ++r) {
-                const StepParam p = s_param[slot * kTileVoxels + warp * kVoxelsPerWarp + r * G + g];
-                if (p.row < 0 || !frames_ok) continue;
+                if (((wmask >> (r * G)) & kGroupMask) == 0u) continue;  // no voxel of this round is valid
+                if (!((wmask >> (r * G + g)) & 1u)) continue;
+                const StepParam p = prm[r * G];
                 uint2 ta, tb, tc;
                 if (mode == 1) {
-                    const unsigned char* q = win + ((p.row - lo) * FC + sub * VF) * kEsz;
-                    constexpr int kRowBytes = FC * kEsz;
+                    const unsigned char* q = win + (p.row - lo) * kRowBytes;
                     if constexpr (INTERP == kNearest) {
                         ta = *reinterpret_cast<const uint2*>(q);
                     } else if constexpr (INTERP == kLinear) {
                         ta = *reinterpret_cast<const uint2*>(q);
-                        tb = *reinterpret_cast<const uint2*>(q + p.step * kRowBytes);
+                        tb = *reinterpret_cast<const uint2*>(q + (p.w > 0.0f ? kRowBytes : 0));
                     } else {
                         ta = *reinterpret_cast<const uint2*>(q - kRowBytes);
                         tb = *reinterpret_cast<const uint2*>(q);
                         tc = *reinterpret_cast<const uint2*>(q + kRowBytes);
                     }
                 } else {
-                    const T* q = grow + static_cast<int64_t>(p.row) * n_frames + frame0;
+                    const T* q = grow + static_cast<int64_t>(p.row) * n_frames;
                     if constexpr (INTERP == kNearest) {
                         ta = __ldg(reinterpret_cast<const uint2*>(q));
                     } else if constexpr (INTERP == kLinear) {
                         ta = __ldg(reinterpret_cast<const uint2*>(q));
-                        tb = __ldg(reinterpret_cast<const uint2*>(q + p.step * n_frames));
+                        tb = __ldg(reinterpret_cast<const uint2*>(q + (p.w > 0.0f ? n_frames : 0)));
                     } else {
                         ta = __ldg(reinterpret_cast<const uint2*>(q - n_frames));
                         tb = __ldg(reinterpret_cast<const uint2*>(q));
@@ -472,20 +520,38 @@ __global__ void __launch_bounds__(kStagedThreads, 1)
                 Vec8<S>::unpack(ta, va);
                 if constexpr (INTERP != kNearest) Vec8<S>::unpack(tb, vb);
                 if constexpr (INTERP == kQuadratic) Vec8<S>::unpack(tc, vc);
+                float wm = 0.f, w0 = 0.f, wp = 0.f;
+                if constexpr (INTERP == kQuadratic) {
+                    const float hx = __fmul_rn(0.5f, p.w);
+                    const float qq = __fmul_rn(hx, p.w);
+                    wm = __fsub_rn(qq, hx);
+                    w0 = __fmaf_rn(-2.0f, qq, 1.0f);
+                    wp = __fadd_rn(qq, hx);
+                }
 #pragma unroll
                 for (int q = 0; q < NP; ++q) {
                     float2 v;
                     if constexpr (INTERP == kNearest) {
                         v = va[q];
                     } else if constexpr (INTERP == kLinear) {
-                        v = fma2(make_float2(p.w0, p.w0), sub2(vb[q], va[q]), va[q]);  // a + t (b - a)
+                        if constexpr (kCplx) {
+                            v.x = __fmaf_rn(p.w, __fsub_rn(vb[q].x, va[q].x), va[q].x);  // a + t (b - a)
+                            v.y = __fmaf_rn(p.w, __fsub_rn(vb[q].y, va[q].y), va[q].y);
+                        } else {
+                            v = fma2(make_float2(p.w, p.w), sub2(vb[q], va[q]), va[q]);
+                        }
                     } else {
-                        v = fma2(make_float2(p.w2, p.w2), vc[q],
-                                 fma2(make_float2(p.w0, p.w0), va[q], mul2(make_float2(p.w1, p.w1), vb[q])));
+                        if constexpr (kCplx) {
+                            v.x = __fmaf_rn(wp, vc[q].x, __fmaf_rn(wm, va[q].x, __fmul_rn(w0, vb[q].x)));
+                            v.y = __fmaf_rn(wp, vc[q].y, __fmaf_rn(wm, va[q].y, __fmul_rn(w0, vb[q].y)));
+                        } else {
+                            v = fma2(make_float2(wp, wp), vc[q],
+                                     fma2(make_float2(wm, wm), va[q], mul2(make_float2(w0, w0), vb[q])));
+                        }
                     }
-                    if (kCplx) {
-                        acc[r][q] = fma2(v, make_float2(p.cw, p.cw), acc[r][q]);
-                        acc[r][q] = fma2(make_float2(v.y, v.x), make_float2(-p.sw, p.sw), acc[r][q]);
+                    if constexpr (kCplx) {
+                        acc[r][q].x = __fmaf_rn(v.x, p.cw, __fmaf_rn(-v.y, p.sw, acc[r][q].x));
+                        acc[r][q].y = __fmaf_rn(v.y, p.cw, __fmaf_rn(v.x, p.sw, acc[r][q].y));
                     } else {
                         acc[r][q] = fma2(v, make_float2(p.cw, p.cw), acc[r][q]);
                     }
@@ -500,14 +566,20 @@ __global__ void __launch_bounds__(kStagedThreads, 1)
         mbar_wait(&s_bar[0], phase[0] ^ 1u);
         mbar_wait(&s_bar[1], phase[1] ^ 1u);
         if (tid == 0) atomicOr(st.status, 1);
-        return;
+        return false;
+    }
+    // No copy is in flight: retire the barriers so the next tile of a persistent CTA can
+    // initialise them again.
+    if (tid == 0) {
+        mbar_inval(&s_bar[0]);
+        mbar_inval(&s_bar[1]);
     }
 
     // ---- write the tile's sums: lane (g, sub) holds frames frame0 .. frame0 + VF - 1
-    if (!frames_ok) return;
+    if (!frames_ok) return true;
 #pragma unroll
     for (int r = 0; r < ROUNDS; ++r) {
-        const int64_t v = tile_voxel(a, st, blockIdx.x, warp * kVoxelsPerWarp + r * G + g);
+        const int64_t v = tile_voxel(a, st, tile, warp * kVoxelsPerWarp + r * G + g);
         if (v < 0) continue;
         if constexpr (kCplx) {
             float2* o = static_cast<float2*>(a.out) + v * n_frames + frame0;
@@ -535,13 +607,23 @@ __global__ void __launch_bounds__(kStagedThreads, 1)
             }
         }
     }
+    return true;
+}
+
+template <int S, int INTERP, int LV>
+__global__ void __launch_bounds__(kStagedThreads, 3)
+    das_staged_kernel(const __grid_constant__ DasArgs a, const __grid_constant__ StagedArgs st,
+                      const __grid_constant__ CUtensorMap tmap) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    staged_tile<S, INTERP, LV>(a, st, &tmap, blockIdx.x, blockIdx.y, smem);
 }
 
 // Shared memory needed by one CTA.
-inline size_t staged_smem_bytes(int window_rows, int frame_chunk, int esz) {
+inline size_t staged_smem_bytes(int window_rows, int frame_chunk, int esz, int n_tx) {
     const size_t window = static_cast<size_t>(window_rows) * frame_chunk * esz;
-    return 2 * window + 3 * kTileVoxels * sizeof(StepParam) + kMaxElemBlock * sizeof(int) +
-           (3 * kStagedWarps * 2 + 3 + 3 + kStagedWarps + 1) * sizeof(int) + kStagedWarps * 5 * sizeof(float) + 8 +
+    const size_t pref = n_tx <= kMaxPrefetchTx ? static_cast<size_t>(n_tx) * kTileVoxels * sizeof(float) : 0;
+    return 2 * window + 3 * kTileVoxels * sizeof(StepParam) + pref + kMaxElemBlock * sizeof(int) +
+           (3 * 4 * 2 + 3 * 4 + 3 + 3 + kStagedWarps) * sizeof(int) + kStagedWarps * 5 * sizeof(float) + 8 +
            2 * sizeof(uint64_t);
 }
 

@@ -4,12 +4,14 @@
 
 #include <algorithm>
 #include <atomic>
+#include <cmath>
 #include <cstdarg>
 #include <cstddef>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <vector>
 
 #include "das_launch.cuh"
 #include "mach_b200.h"
@@ -158,7 +160,9 @@ constexpr int kMaxTxChunk = 32;  // lane-voxel kernel: 32 x 128 voxels x 4 B = 1
 struct Plan {
     LaunchPlan lp{};
     StagedArgs st{};
+    EnsembleArgs ea{};
     bool staged = false;
+    bool ensemble = false;
 };
 
 int next_pow2(int x) {
@@ -191,36 +195,110 @@ bool grid_matches(const mach_b200_options& o, uint64_t n_vox) {
     return a > 0 && b > 0 && c > 0 && static_cast<uint64_t>(a * b * c) == n_vox;
 }
 
+// Ensemble kernel plan (lanes = frames, windows in tensor memory), or false when the job
+// does not meet its conditions: nearest / linear taps, a TMA-able channel (16-byte aligned
+// base, row pitch a multiple of 16 bytes), fewer than 2^31 voxels.
+bool plan_ensemble(int storage, int interp, uint64_t n_vox, uint32_t n_frames, uint32_t n_tx, const void* channel,
+                   bool channel_on_device, const mach_b200_options& o, Plan& p) {
+    const int esz = static_cast<int>(storage_bytes(storage));
+    const bool cplx = (storage & 1) != 0;
+    if (interp != kNearest && interp != kLinear) return false;
+    if (n_vox == 0 || n_vox > 0x7fffffffull || n_frames == 0) return false;
+    if ((static_cast<uint64_t>(n_frames) * esz) % 16 != 0) return false;
+    if (channel_on_device && reinterpret_cast<uintptr_t>(channel) % 16 != 0) return false;
+    if (tensor_map_encoder() == nullptr) return false;
+    const int lwb = (storage == kC64 || storage == kF32) ? 8 : 4;  // bytes of one lane word
+    const int frames_per_lane = cplx ? 1 : 2;
+    int w = o.window_rows > 0 ? o.window_rows : 48;
+    w = std::min(kEnsMaxWindow, std::max(16, (w + 15) & ~15));
+    EnsembleArgs& ea = p.ea;
+    ea.window_rows = w;
+    ea.n_fblocks = static_cast<int32_t>((n_frames + 32u * frames_per_lane - 1) / (32u * frames_per_lane));
+    ea.box_x = 32 * lwb / esz;
+    ea.tmem_cols = static_cast<uint32_t>(std::max(32, next_pow2(4 * w)));
+    StagedArgs& st = p.st;
+    if (grid_matches(o, n_vox)) {
+        st.grid_slow = o.grid_shape[0];
+        st.grid_mid = o.grid_shape[1];
+        st.grid_fast = o.grid_shape[2];
+        st.tile_fast = 4;  // along the contiguous axis (depth, for a scan ordered depth-fastest)
+        st.tile_mid = st.grid_mid <= 1 ? 1 : 4;
+        st.tile_slow = st.grid_mid <= 1 ? 32 : 8;
+        st.tiles_fast = (st.grid_fast + st.tile_fast - 1) / st.tile_fast;
+        st.tiles_mid = (st.grid_mid + st.tile_mid - 1) / st.tile_mid;
+        const int64_t tiles = static_cast<int64_t>(st.tiles_fast) * st.tiles_mid *
+                              ((st.grid_slow + st.tile_slow - 1) / st.tile_slow);
+        ea.n_tiles = static_cast<int32_t>(tiles);
+    } else {
+        st.grid_fast = 0;
+        ea.n_tiles = static_cast<int32_t>((n_vox + kEnsTileVoxels - 1) / kEnsTileVoxels);
+    }
+    if (static_cast<int64_t>(ea.n_tiles) * ea.n_fblocks > 0x7fffffffll) return false;
+    st.use_tma = 1;
+    st.window_rows = w;
+    const int n_pref = n_tx <= static_cast<uint32_t>(kEnsMaxPrefetchTx) ? static_cast<int>(n_tx) : 0;
+    ea.team_bytes = ensemble_team_bytes(w, lwb, n_pref);
+    p.ensemble = true;
+    p.staged = false;
+    p.lp.kind = kKindEnsemble;
+    p.lp.block = dim3(kEnsThreads, 1, 1);
+    p.lp.grid = dim3(1, 1, 1);  // persistent; the launcher sizes it
+    p.lp.passes = 1;
+    p.lp.tx_chunk = 1;
+    p.lp.lanes_per_voxel = 32;
+    p.lp.smem = static_cast<size_t>(kEnsTeams) * ea.team_bytes;
+    return true;
+}
+
 Plan plan_launch(int storage, uint64_t n_vox, uint32_t n_frames, uint32_t n_tx, const void* channel,
-                 bool channel_on_device, const mach_b200_options& o) {
+                 bool channel_on_device, const mach_b200_options& o, int interp = -1) {
     Plan p;
     const int esz = static_cast<int>(storage_bytes(storage));
     const int vf = 8 / esz;
     int kind = o.kernel;
+    // Ensemble kernel: asked for, or automatic for many frames on a known voxel grid
+    // (interp < 0: a caller that cannot run it, e.g. a batch).
+    if (interp >= 0) {
+        const bool many = n_frames >= ((storage & 1) ? 32u : 64u);
+        if (kind == MACH_B200_KERNEL_ENSEMBLE ||
+            (kind == MACH_B200_KERNEL_AUTO && many && grid_matches(o, n_vox))) {
+            if (plan_ensemble(storage, interp, n_vox, n_frames, n_tx, channel, channel_on_device, o, p)) return p;
+            p = Plan{};
+        }
+    }
+    if (kind == MACH_B200_KERNEL_ENSEMBLE) kind = MACH_B200_KERNEL_AUTO;
     // Host channel data is staged into fresh (aligned) device buffers.
     const bool vec_ok =
         n_frames % static_cast<uint32_t>(vf) == 0 && (!channel_on_device || reinterpret_cast<uintptr_t>(channel) % 8 == 0);
+    // 16 frames per sample as 16-byte vectors: rows must be 16-byte multiples and aligned.
+    const bool lane16_ok = n_frames == 16 && (16u * esz) % 16u == 0 &&
+                           (!channel_on_device || reinterpret_cast<uintptr_t>(channel) % 16 == 0);
     if (kind == MACH_B200_KERNEL_AUTO) {
-        kind = n_frames <= 8 ? MACH_B200_KERNEL_LANE_VOXEL : (vec_ok ? MACH_B200_KERNEL_STAGED : MACH_B200_KERNEL_WARP);
+        kind = (n_frames <= 8 || lane16_ok) ? MACH_B200_KERNEL_LANE_VOXEL
+                                            : (vec_ok ? MACH_B200_KERNEL_STAGED : MACH_B200_KERNEL_WARP);
     }
-    if (kind == MACH_B200_KERNEL_LANE_VOXEL && n_frames > 8) kind = MACH_B200_KERNEL_WARP;
+    if (kind == MACH_B200_KERNEL_LANE_VOXEL && n_frames > 8 && !lane16_ok) kind = MACH_B200_KERNEL_WARP;
     if (kind == MACH_B200_KERNEL_STAGED && !vec_ok) kind = MACH_B200_KERNEL_WARP;
 
     if (kind == MACH_B200_KERNEL_LANE_VOXEL) {
-        p.lp.kind = n_frames <= 1 ? kKindLaneVoxel1 : kKindLaneVoxelN;
+        p.lp.kind = n_frames <= 1 ? kKindLaneVoxel1 : (n_frames == 16 ? kKindLaneVoxel16 : kKindLaneVoxelN);
         p.lp.passes = static_cast<int>(n_frames);
         const int chunk = o.tx_chunk > 0 ? o.tx_chunk : kMaxTxChunk;
         const uint32_t chunks = std::max<uint32_t>(1u, (n_tx + chunk - 1) / chunk);
         p.lp.tx_chunk = static_cast<int>(std::max<uint32_t>(1u, (n_tx + chunks - 1) / chunks));
         p.lp.block = dim3(kLaneVoxelThreads, 1, 1);
         p.lp.grid = dim3(static_cast<unsigned>((n_vox + kLaneVoxelThreads - 1) / kLaneVoxelThreads), 1, 1);
-        p.lp.smem = static_cast<size_t>(p.lp.tx_chunk) * kLaneVoxelThreads * sizeof(float);
+        // split mode stages three words per (transmit, voxel): base, fraction, phase cycles
+        p.lp.smem = static_cast<size_t>(p.lp.tx_chunk) * kLaneVoxelThreads * sizeof(float) *
+                    ((o.flags & MACH_B200_FLAG_SPLIT_DELAY) ? 3 : 1);
         return p;
     }
     if (kind == MACH_B200_KERNEL_STAGED) {
         const int lanes_needed = static_cast<int>((n_frames + vf - 1) / vf);
         int lv = o.lanes_per_voxel > 0 ? o.lanes_per_voxel : std::min(32, std::max(4, next_pow2(lanes_needed)));
         if (lv != 4 && lv != 8 && lv != 16 && lv != 32) lv = 32;
+        // two float2 pairs per lane vector (16-bit real, any 16-bit or half complex): at most 16 lanes
+        if (storage != kC64 && storage != kF32) lv = std::min(lv, 16);
         const int fc = lv * vf;
         int w = o.window_rows > 0 ? o.window_rows : (fc * esz >= 256 ? 64 : 128);
         w = std::min(256, std::max(4, (w + 3) & ~3));  // multiple of 4 keeps both windows 128-byte aligned
@@ -246,7 +324,7 @@ Plan plan_launch(int storage, uint64_t n_vox, uint32_t n_frames, uint32_t n_tx, 
                         (static_cast<uint64_t>(n_frames) * esz) % 16 == 0 && tensor_map_encoder() != nullptr)
                            ? 1
                            : 0;
-        p.lp.smem = staged_smem_bytes(w, fc, esz);
+        p.lp.smem = staged_smem_bytes(w, fc, esz, static_cast<int>(n_tx));
         return p;
     }
     // warp-per-voxel multi-frame kernel (any frame count)
@@ -295,6 +373,21 @@ cudaError_t dispatch(int storage, const DasArgs& a, int interp, const Plan& plan
     case S:                                                                             \
         return plan.staged ? launch_das_staged<S>(a, plan.st, map, interp, plan.lp, st) \
                            : launch_das<S>(a, interp, plan.lp, st);
+    if (plan.ensemble) {
+#define MACH_B200_ECASE(S) \
+    case S: return launch_das_ensemble<S>(a, plan.st, plan.ea, map, interp, plan.lp.smem, st);
+        switch (storage) {
+            MACH_B200_ECASE(kF32)
+            MACH_B200_ECASE(kC64)
+            MACH_B200_ECASE(kF16)
+            MACH_B200_ECASE(kCF16)
+            MACH_B200_ECASE(kBF16)
+            MACH_B200_ECASE(kCBF16)
+            MACH_B200_ECASE(kI16)
+            default: return launch_das_ensemble<kCI16>(a, plan.st, plan.ea, map, interp, plan.lp.smem, st);
+        }
+#undef MACH_B200_ECASE
+    }
     switch (storage) {
         MACH_B200_CASE(kF32)
         MACH_B200_CASE(kC64)
@@ -328,8 +421,8 @@ int dispatch_split(int storage, DasArgs a, int interp, const Plan& plan, cudaStr
         b.accumulate = t0 == 0 ? a.accumulate : 1;
         CUtensorMap map;
         std::memset(&map, 0, sizeof(map));
-        if (plan.staged && plan.st.use_tma && b.n_tx > 0) {
-            const int fc = plan.lp.lanes_per_voxel * static_cast<int>(8 / esz);
+        if ((plan.staged || plan.ensemble) && plan.st.use_tma && b.n_tx > 0) {
+            const int fc = plan.ensemble ? plan.ea.box_x : plan.lp.lanes_per_voxel * static_cast<int>(8 / esz);
             const int rc = encode_channel_map(&map, storage, b.channel,
                                               static_cast<uint64_t>(b.n_tx) * a.n_rx * a.n_samples, a.n_frames, fc,
                                               plan.st.window_rows);
@@ -393,13 +486,49 @@ int check_status(DeviceState* dev, cudaStream_t stream) {
     return MACH_B200_OK;
 }
 
-int compound_impl(int32_t storage, const void* channel_data, const float* rx_coords_m, const float* scan_coords_m,
-                  const float* tx_wave_arrivals_s, void* out, uint32_t n_tx, uint32_t n_rx, uint32_t n_samples,
-                  uint64_t n_scan, uint32_t n_frames, float f_number, float rx_start_s, float sampling_freq_hz,
-                  float sound_speed_m_s, float modulation_freq_hz, float tukey_alpha, int32_t interp_type,
-                  float channel_scale, cudaStream_t stream, const mach_b200_options& opt) {
-    g_error.clear();
-    const uint32_t flags = opt.flags;
+// Launch arguments shared by every kernel family (FP32 constants rounded on the host the
+// way mach's launcher rounds them, split-delay FP64 constants).
+DasArgs make_args(const float* rx_coords_m, const float* scan_coords_m, uint64_t n_scan, uint32_t n_rx,
+                  uint32_t n_samples, uint32_t n_frames, float f_number, float rx_start_s, float sampling_freq_hz,
+                  float sound_speed_m_s, float modulation_freq_hz, float tukey_alpha, float channel_scale, bool cplx,
+                  uint32_t flags) {
+    DasArgs a{};
+    a.rx = rx_coords_m;
+    a.scan = scan_coords_m;
+    a.n_vox = static_cast<int64_t>(n_scan);
+    a.n_rx = static_cast<int32_t>(n_rx);
+    a.n_samples = static_cast<int32_t>(n_samples);
+    a.n_frames = static_cast<int32_t>(n_frames);
+    a.row_stride = static_cast<int64_t>(n_samples) * n_frames;
+    a.inv_c = 1.0f / sound_speed_m_s;  // kernel.cu:750, FP32 on the host
+    a.fs = sampling_freq_hz;
+    a.t0 = rx_start_s;
+    a.two_f_number = 2.0f * f_number;
+    a.alpha = tukey_alpha;
+    a.one_minus_alpha = 1.0f - tukey_alpha;
+    a.mod_rad = (2.0f * kPi) * modulation_freq_hz;  // kernel.cu:571
+    a.scale = channel_scale;
+    a.hi_nearest = static_cast<float>(n_samples) - 0.5f;
+    a.hi_linear = static_cast<float>(n_samples - 1u);
+    a.hi_quadratic = static_cast<float>(n_samples) - 2.0f;
+    a.apod = tukey_alpha > 0.0f;
+    a.rotate = cplx && modulation_freq_hz != 0.0f;
+    a.split = (flags & MACH_B200_FLAG_SPLIT_DELAY) != 0u ? 1 : 0;
+    a.fs_d = sampling_freq_hz;
+    a.t0_d = rx_start_s;
+    a.fmod_d = modulation_freq_hz;
+    a.fs_over_c = static_cast<double>(sampling_freq_hz) / static_cast<double>(sound_speed_m_s);
+    a.fmod_over_c = static_cast<double>(modulation_freq_hz) / static_cast<double>(sound_speed_m_s);
+    const double start = -static_cast<double>(rx_start_s) * static_cast<double>(sampling_freq_hz);
+    const double b = std::floor(start);
+    a.start_base = static_cast<int32_t>(std::max(-2.0e9, std::min(2.0e9, b)));
+    a.start_frac = static_cast<float>(start - b);
+    return a;
+}
+
+// Argument checks shared by every entry point (messages follow mach where it has one).
+int check_args(int32_t storage, int32_t interp_type, float tukey_alpha, uint32_t n_tx, uint32_t n_rx,
+               uint32_t n_samples, uint64_t n_scan, uint32_t n_frames) {
     if (storage < kF32 || storage > kCI16) return fail(MACH_B200_ERR_VALUE, "unknown storage code %d", storage);
     if (interp_type < kNearest || interp_type > kQuadratic) {
         return fail(MACH_B200_ERR_VALUE,
@@ -408,12 +537,6 @@ int compound_impl(int32_t storage, const void* channel_data, const float* rx_coo
     // Same range check and message as mach (src/mach/kernel.cu:745-748).
     if (!(tukey_alpha >= 0.0f && tukey_alpha <= 1.0f)) {
         return fail(MACH_B200_ERR_VALUE, "Error: tukey_alpha must be in range [0, 1], but got %f", tukey_alpha);
-    }
-    if (n_scan == 0 || n_frames == 0) return MACH_B200_OK;  // empty output: nothing to write
-    if (!out || !scan_coords_m) return fail(MACH_B200_ERR_VALUE, "out and scan_coords_m must not be NULL");
-    const bool need_channel = n_tx > 0 && n_rx > 0 && n_samples > 0;
-    if (need_channel && (!channel_data || !rx_coords_m || !tx_wave_arrivals_s)) {
-        return fail(MACH_B200_ERR_VALUE, "channel_data, rx_coords_m and tx_wave_arrivals_s must not be NULL");
     }
     if (n_frames > 1000000u) return fail(MACH_B200_ERR_VALUE, "n_frames %u is too large (at most 1000000)", n_frames);
     // Sample positions are rounded with FP32 adds that are exact below 2^22.
@@ -426,6 +549,24 @@ int compound_impl(int32_t storage, const void* channel_data, const float* rx_coo
     if (n_rx > 0x7fffffffu || n_tx > 0x7fffffffu) return fail(MACH_B200_ERR_VALUE, "n_rx / n_tx too large");
     if (n_scan > 0x7fffffffull * 4ull) {
         return fail(MACH_B200_ERR_VALUE, "n_scan %llu is too large", static_cast<unsigned long long>(n_scan));
+    }
+    return MACH_B200_OK;
+}
+
+int compound_impl(int32_t storage, const void* channel_data, const float* rx_coords_m, const float* scan_coords_m,
+                  const float* tx_wave_arrivals_s, void* out, uint32_t n_tx, uint32_t n_rx, uint32_t n_samples,
+                  uint64_t n_scan, uint32_t n_frames, float f_number, float rx_start_s, float sampling_freq_hz,
+                  float sound_speed_m_s, float modulation_freq_hz, float tukey_alpha, int32_t interp_type,
+                  float channel_scale, cudaStream_t stream, const mach_b200_options& opt) {
+    g_error.clear();
+    const uint32_t flags = opt.flags;
+    int rc0 = check_args(storage, interp_type, tukey_alpha, n_tx, n_rx, n_samples, n_scan, n_frames);
+    if (rc0) return rc0;
+    if (n_scan == 0 || n_frames == 0) return MACH_B200_OK;  // empty output: nothing to write
+    if (!out || !scan_coords_m) return fail(MACH_B200_ERR_VALUE, "out and scan_coords_m must not be NULL");
+    const bool need_channel = n_tx > 0 && n_rx > 0 && n_samples > 0;
+    if (need_channel && (!channel_data || !rx_coords_m || !tx_wave_arrivals_s)) {
+        return fail(MACH_B200_ERR_VALUE, "channel_data, rx_coords_m and tx_wave_arrivals_s must not be NULL");
     }
 
     int device = 0;
@@ -446,29 +587,11 @@ int compound_impl(int32_t storage, const void* channel_data, const float* rx_coo
     const size_t esz = storage_bytes(storage);
     const size_t out_bytes = static_cast<size_t>(n_scan) * n_frames * (cplx ? 8 : 4);
 
-    DasArgs a{};
-    a.rx = rx_coords_m;
-    a.scan = scan_coords_m;
-    a.n_vox = static_cast<int64_t>(n_scan);
-    a.n_rx = static_cast<int32_t>(need_channel ? n_rx : 0);
-    a.n_samples = static_cast<int32_t>(n_samples);
-    a.n_frames = static_cast<int32_t>(n_frames);
-    a.row_stride = static_cast<int64_t>(n_samples) * n_frames;
-    a.inv_c = 1.0f / sound_speed_m_s;  // kernel.cu:750, FP32 on the host
-    a.fs = sampling_freq_hz;
-    a.t0 = rx_start_s;
-    a.two_f_number = 2.0f * f_number;
-    a.alpha = tukey_alpha;
-    a.one_minus_alpha = 1.0f - tukey_alpha;
-    a.mod_rad = (2.0f * kPi) * modulation_freq_hz;  // kernel.cu:571
-    a.scale = channel_scale;
-    a.hi_nearest = static_cast<float>(n_samples) - 0.5f;
-    a.hi_linear = static_cast<float>(n_samples - 1u);
-    a.hi_quadratic = static_cast<float>(n_samples) - 2.0f;
-    a.apod = tukey_alpha > 0.0f;
-    a.rotate = cplx && modulation_freq_hz != 0.0f;
+    DasArgs a = make_args(rx_coords_m, scan_coords_m, n_scan, need_channel ? n_rx : 0, n_samples, n_frames, f_number,
+                          rx_start_s, sampling_freq_hz, sound_speed_m_s, modulation_freq_hz, tukey_alpha,
+                          channel_scale, cplx, flags);
     const bool overwrite = (flags & MACH_B200_FLAG_OVERWRITE) != 0u || r_out != kOnDevice;
-    Plan plan = plan_launch(storage, n_scan, n_frames, n_tx, channel_data, r_ch == kOnDevice, opt);
+    Plan plan = plan_launch(storage, n_scan, n_frames, n_tx, channel_data, r_ch == kOnDevice, opt, interp_type);
     plan.st.status = dev->status;
     a.frame_passes = plan.lp.passes;
     a.tx_chunk = plan.lp.tx_chunk;
@@ -484,7 +607,7 @@ int compound_impl(int32_t storage, const void* channel_data, const float* rx_coo
         if ((rc = dispatch_split(storage, a, interp_type, plan, stream))) return rc;
         if (!(flags & MACH_B200_FLAG_ASYNC)) {
             MACH_B200_CUDA_TRY(cudaStreamSynchronize(stream));
-            if (plan.staged) return check_status(dev, stream);
+            if (plan.staged || plan.ensemble) return check_status(dev, stream);
         }
         return MACH_B200_OK;
     }
@@ -577,7 +700,7 @@ int compound_impl(int32_t storage, const void* channel_data, const float* rx_coo
     }
     // Host buffers are in use until the stream drains: always synchronous here.
     MACH_B200_CUDA_TRY(cudaStreamSynchronize(stream));
-    if (plan.staged) return check_status(dev, stream);
+    if (plan.staged || plan.ensemble) return check_status(dev, stream);
     return MACH_B200_OK;
 }
 
@@ -589,6 +712,248 @@ mach_b200_options default_options(uint32_t flags) {
     return o;
 }
 
+
+// ---------------------------------------------------------------- batches
+
+}  // namespace
+
+struct mach_b200_batch {
+    int device = 0;
+    uint32_t max_jobs = 0;
+    static constexpr int kMaxGroups = 32;
+    // pinned host tables (filled on the host, copied by the stream)
+    BatchJob* h_jobs = nullptr;
+    int64_t* h_begin = nullptr;
+    BatchHeader* h_hdr = nullptr;
+    // device tables
+    BatchJob* d_jobs = nullptr;
+    int64_t* d_begin = nullptr;
+    BatchHeader* d_hdr = nullptr;
+    unsigned long long* d_counters = nullptr;
+    cudaEvent_t copied = nullptr;  // host tables may be rewritten once this has passed
+    bool pending = false;
+};
+
+namespace {
+
+struct GroupKey {
+    int family;  // 0 lane-voxel, 1 staged
+    int storage;
+    int interp;
+    int variant;  // lane-voxel frame class (1, 0, 16) or staged lanes per voxel
+    int split;
+    bool operator==(const GroupKey& o) const {
+        return family == o.family && storage == o.storage && interp == o.interp && variant == o.variant &&
+               split == o.split;
+    }
+};
+
+cudaError_t launch_group(const GroupKey& k, const PersistentLaunch& pl, cudaStream_t st) {
+#define MACH_B200_GCASE(S)                                                                                   \
+    case S:                                                                                                   \
+        return k.family == 0 ? launch_lane_voxel_persistent<S>(k.interp, k.variant, k.split != 0, pl, st)     \
+                             : launch_staged_persistent<S>(k.interp, k.variant, pl, st);
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    switch (k.storage) {
+        MACH_B200_GCASE(kF32)
+        MACH_B200_GCASE(kC64)
+        MACH_B200_GCASE(kF16)
+        MACH_B200_GCASE(kCF16)
+        MACH_B200_GCASE(kBF16)
+        MACH_B200_GCASE(kCBF16)
+        MACH_B200_GCASE(kI16)
+        default:
+            return k.family == 0 ? launch_lane_voxel_persistent<kCI16>(k.interp, k.variant, k.split != 0, pl, st)
+                                 : launch_staged_persistent<kCI16>(k.interp, k.variant, pl, st);
+    }
+#undef MACH_B200_GCASE
+}
+
+void batch_free(mach_b200_batch* b) {
+    if (!b) return;
+    if (b->copied) {
+        cudaEventSynchronize(b->copied);
+        cudaEventDestroy(b->copied);
+    }
+    cudaFreeHost(b->h_jobs);
+    cudaFreeHost(b->h_begin);
+    cudaFreeHost(b->h_hdr);
+    cudaFree(b->d_jobs);
+    cudaFree(b->d_begin);
+    cudaFree(b->d_hdr);
+    cudaFree(b->d_counters);
+    delete b;
+}
+
+int batch_create(uint32_t max_jobs, mach_b200_batch** out) {
+    g_error.clear();
+    if (!out) return fail(MACH_B200_ERR_VALUE, "batch pointer must not be NULL");
+    *out = nullptr;
+    if (max_jobs == 0 || max_jobs > (1u << 20)) return fail(MACH_B200_ERR_VALUE, "max_jobs must be in [1, 2^20]");
+    auto* b = new mach_b200_batch();
+    b->max_jobs = max_jobs;
+    const size_t G = mach_b200_batch::kMaxGroups;
+    cudaError_t e = cudaGetDevice(&b->device);
+    if (e == cudaSuccess) e = cudaMallocHost(&b->h_jobs, sizeof(BatchJob) * max_jobs);
+    if (e == cudaSuccess) e = cudaMallocHost(&b->h_begin, sizeof(int64_t) * max_jobs);
+    if (e == cudaSuccess) e = cudaMallocHost(&b->h_hdr, sizeof(BatchHeader) * G);
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_jobs, sizeof(BatchJob) * max_jobs);
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_begin, sizeof(int64_t) * max_jobs);
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_hdr, sizeof(BatchHeader) * G);
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_counters, sizeof(unsigned long long) * G);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->copied, cudaEventDisableTiming);
+    if (e != cudaSuccess) {
+        batch_free(b);
+        return fail(MACH_B200_ERR_CUDA, "batch context allocation failed: %s", cudaGetErrorString(e));
+    }
+    *out = b;
+    return MACH_B200_OK;
+}
+
+int batch_run(mach_b200_batch* b, const mach_b200_job* jobs, uint32_t n_jobs, cudaStream_t stream, uint32_t flags) {
+    g_error.clear();
+    if (!b) return fail(MACH_B200_ERR_VALUE, "batch context is NULL");
+    if (n_jobs > b->max_jobs) return fail(MACH_B200_ERR_VALUE, "%u jobs exceed the context's %u", n_jobs, b->max_jobs);
+    if (n_jobs && !jobs) return fail(MACH_B200_ERR_VALUE, "jobs must not be NULL");
+    int device = 0;
+    MACH_B200_CUDA_TRY(cudaGetDevice(&device));
+    if (device != b->device) return fail(MACH_B200_ERR_DEVICE, "batch context belongs to device %d", b->device);
+    DeviceState* dev = nullptr;
+    int rc;
+    if ((rc = device_state(device, &dev))) return rc;
+
+    // The previous run's table copies read the pinned tables: wait before rewriting them.
+    if (b->pending) {
+        MACH_B200_CUDA_TRY(cudaEventSynchronize(b->copied));
+        b->pending = false;
+    }
+
+    // ---- plan every job, assign it to a group (kernel signature)
+    GroupKey keys[mach_b200_batch::kMaxGroups];
+    int n_groups = 0;
+    std::vector<int> group_of(n_jobs), order;
+    std::vector<Plan> plans(n_jobs);
+    for (uint32_t i = 0; i < n_jobs; ++i) {
+        const mach_b200_job& j = jobs[i];
+        if ((rc = check_args(j.storage, j.interp_type, j.tukey_alpha, j.n_tx, j.n_rx, j.n_samples, j.n_scan,
+                             j.n_frames))) {
+            return fail(MACH_B200_ERR_VALUE, "job %u: %s", i, g_error.c_str());
+        }
+        if (static_cast<uint64_t>(j.n_tx) * j.n_rx * j.n_samples * j.n_frames >= (uint64_t{1} << 31)) {
+            return fail(MACH_B200_ERR_VALUE, "job %u: channel data above 2^31 samples; use mach_b200_beamform_ex", i);
+        }
+        const void* ptrs[5] = {j.channel_data, j.rx_coords_m, j.scan_coords_m, j.tx_wave_arrivals_s, j.out};
+        for (const void* p : ptrs) {
+            Residency r;
+            if (p && (rc = residency(p, device, &r, "a batch buffer"))) return rc;
+            if (!p || r != kOnDevice) return fail(MACH_B200_ERR_VALUE, "job %u: batch buffers must be device memory", i);
+        }
+        mach_b200_options o = default_options(j.flags);
+        std::memcpy(o.grid_shape, j.grid_shape, sizeof(o.grid_shape));
+        o.kernel = j.kernel == MACH_B200_KERNEL_WARP ? MACH_B200_KERNEL_AUTO : j.kernel;
+        o.tx_chunk = j.tx_chunk;
+        o.window_rows = j.window_rows;
+        o.lanes_per_voxel = j.lanes_per_voxel;
+        plans[i] = plan_launch(j.storage, j.n_scan, j.n_frames, j.n_tx, j.channel_data, true, o);
+        const Plan& p = plans[i];
+        GroupKey k{};
+        if (p.staged) {
+            k = {1, j.storage, j.interp_type, p.lp.lanes_per_voxel, 0};
+        } else if (p.lp.kind == kKindLaneVoxel1 || p.lp.kind == kKindLaneVoxelN || p.lp.kind == kKindLaneVoxel16) {
+            const int fc = p.lp.kind == kKindLaneVoxel1 ? 1 : (p.lp.kind == kKindLaneVoxel16 ? 16 : 0);
+            k = {0, j.storage, j.interp_type, fc, (j.flags & MACH_B200_FLAG_SPLIT_DELAY) ? 1 : 0};
+        } else {
+            return fail(MACH_B200_ERR_VALUE, "job %u: %u frames not a multiple of the storage's lane vector", i,
+                        j.n_frames);
+        }
+        int gi = 0;
+        while (gi < n_groups && !(keys[gi] == k)) ++gi;
+        if (gi == n_groups) {
+            if (n_groups == mach_b200_batch::kMaxGroups) return fail(MACH_B200_ERR_VALUE, "too many kernel signatures");
+            keys[n_groups++] = k;
+        }
+        group_of[i] = gi;
+    }
+
+    // ---- fill the pinned tables, grouped
+    std::vector<int> first(n_groups + 1, 0);
+    for (uint32_t i = 0; i < n_jobs; ++i) ++first[group_of[i] + 1];
+    for (int g = 0; g < n_groups; ++g) first[g + 1] += first[g];
+    std::vector<int> fill(first.begin(), first.end() - 1);
+    std::vector<size_t> smem(n_groups, 0);
+    std::vector<int64_t> items(n_groups, 0);
+    std::vector<int> max_items(n_groups, 0);
+    for (uint32_t i = 0; i < n_jobs; ++i) {
+        const mach_b200_job& j = jobs[i];
+        const int g = group_of[i];
+        const int slot = fill[g]++;
+        BatchJob& bj = b->h_jobs[slot];
+        std::memset(&bj, 0, sizeof(bj));
+        const bool cplx = (j.storage & 1) != 0;
+        const bool need_channel = j.n_tx > 0 && j.n_rx > 0 && j.n_samples > 0;
+        bj.a = make_args(j.rx_coords_m, j.scan_coords_m, j.n_scan, need_channel ? j.n_rx : 0, j.n_samples, j.n_frames,
+                         j.f_number, j.rx_start_s, j.sampling_freq_hz, j.sound_speed_m_s, j.modulation_freq_hz,
+                         j.tukey_alpha, j.channel_scale, cplx, j.flags);
+        bj.a.channel = j.channel_data;
+        bj.a.arrivals = j.tx_wave_arrivals_s;
+        bj.a.out = j.out;
+        bj.a.n_tx = static_cast<int32_t>(need_channel ? j.n_tx : 0);
+        bj.a.accumulate = (j.flags & MACH_B200_FLAG_OVERWRITE) ? 0 : 1;
+        const Plan& p = plans[i];
+        bj.a.frame_passes = p.lp.passes;
+        bj.a.tx_chunk = p.lp.tx_chunk;
+        bj.st = p.st;
+        bj.st.status = dev->status;
+        bj.tiles = static_cast<int32_t>(p.lp.grid.x);
+        bj.chunks = static_cast<int32_t>(p.staged ? p.lp.grid.y : 1);
+        if (p.staged && p.st.use_tma && bj.a.n_tx > 0) {
+            const int fc = p.lp.lanes_per_voxel * static_cast<int>(8 / storage_bytes(j.storage));
+            if ((rc = encode_channel_map(&bj.map, j.storage, j.channel_data,
+                                         static_cast<uint64_t>(j.n_tx) * j.n_rx * j.n_samples, j.n_frames, fc,
+                                         p.st.window_rows))) {
+                return rc;
+            }
+        }
+        const int64_t job_items = static_cast<int64_t>(bj.tiles) * bj.chunks;
+        b->h_begin[slot] = items[g];
+        items[g] += job_items;
+        smem[g] = std::max(smem[g], p.lp.smem);
+    }
+    for (int g = 0; g < n_groups; ++g) {
+        b->h_hdr[g].n_items = items[g];
+        b->h_hdr[g].n_jobs = first[g + 1] - first[g];
+        max_items[g] = static_cast<int>(std::min<int64_t>(items[g], 1 << 30));
+    }
+
+    // ---- copies, counters, one persistent launch per group
+    if (n_jobs) {
+        MACH_B200_CUDA_TRY(cudaMemcpyAsync(b->d_jobs, b->h_jobs, sizeof(BatchJob) * n_jobs, cudaMemcpyHostToDevice, stream));
+        MACH_B200_CUDA_TRY(cudaMemcpyAsync(b->d_begin, b->h_begin, sizeof(int64_t) * n_jobs, cudaMemcpyHostToDevice, stream));
+        MACH_B200_CUDA_TRY(cudaMemcpyAsync(b->d_hdr, b->h_hdr, sizeof(BatchHeader) * n_groups, cudaMemcpyHostToDevice, stream));
+        MACH_B200_CUDA_TRY(cudaMemsetAsync(b->d_counters, 0, sizeof(unsigned long long) * n_groups, stream));
+        // While capturing a graph the copies run at replay time, from the tables as they are then.
+        cudaStreamCaptureStatus capturing = cudaStreamCaptureStatusNone;
+        MACH_B200_CUDA_TRY(cudaStreamIsCapturing(stream, &capturing));
+        if (capturing == cudaStreamCaptureStatusNone) {
+            MACH_B200_CUDA_TRY(cudaEventRecord(b->copied, stream));
+            b->pending = true;
+        }
+    }
+    bool any_staged = false;
+    for (int g = 0; g < n_groups; ++g) {
+        if (items[g] == 0) continue;
+        PersistentLaunch pl{b->d_hdr + g, b->d_jobs + first[g], b->d_begin + first[g], b->d_counters + g, smem[g],
+                            max_items[g]};
+        any_staged |= keys[g].family == 1;
+        MACH_B200_CUDA_TRY(launch_group(keys[g], pl, stream));
+    }
+    if (!(flags & MACH_B200_FLAG_ASYNC)) {
+        MACH_B200_CUDA_TRY(cudaStreamSynchronize(stream));
+        b->pending = false;
+        if (any_staged) return check_status(dev, stream);
+    }
+    return MACH_B200_OK;
+}
 }  // namespace
 
 extern "C" {
@@ -644,6 +1009,15 @@ int mach_b200_beamform_ex(int32_t storage, const void* channel_data, const float
                          modulation_freq_hz, tukey_alpha, interp_type, channel_scale,
                          static_cast<cudaStream_t>(cuda_stream), o);
 }
+
+int mach_b200_batch_create(uint32_t max_jobs, mach_b200_batch** batch) { return batch_create(max_jobs, batch); }
+
+int mach_b200_batch_run(mach_b200_batch* batch, const mach_b200_job* jobs, uint32_t n_jobs, void* cuda_stream,
+                        uint32_t flags) {
+    return batch_run(batch, jobs, n_jobs, static_cast<cudaStream_t>(cuda_stream), flags);
+}
+
+void mach_b200_batch_destroy(mach_b200_batch* batch) { batch_free(batch); }
 
 const char* mach_b200_last_error(void) { return g_error.c_str(); }
 

@@ -50,6 +50,7 @@ def beamform(
     window_rows: int = 0,
     lanes_per_voxel: int = 0,
     tx_chunk: int = 0,
+    delay: str = "auto",
 ) -> Any:
     """Beamform and coherently compound ``n_transmits`` transmits.
 
@@ -67,6 +68,11 @@ def beamform(
             Only the voxel-to-CTA assignment depends on it, never the result.
         kernel, window_rows, lanes_per_voxel, tx_chunk: launch tuning (see
             ``mach_b200_options`` in include/mach_b200.h); the autotuner sets them.
+        delay: ``"reference"`` computes delays in FP32 exactly as mach does (bit-identical
+            sample positions); ``"split"`` forms each sample position and phase in FP64 per
+            receive path and per transmit as an integer base + FP32 fraction (more accurate,
+            not bit-identical to mach); ``"auto"`` uses ``"reference"`` for float32/complex64
+            storage and ``"split"`` for reduced-precision storage.
         Other arguments as in :func:`mach_b200.kernel.beamform`.
 
     Returns:
@@ -136,6 +142,12 @@ def beamform(
         )
     all_gpu = all(v.on_cuda for v in (ch, rx, scan, arr, o))
     flags = 0 if (sync or not all_gpu) else _cuda_impl.FLAG_ASYNC
+    if delay == "auto":
+        delay = "reference" if storage in ("f32", "c64") else "split"
+    if delay not in ("reference", "split"):
+        raise ValueError(f"delay must be 'auto', 'reference' or 'split', got {delay!r}")
+    if delay == "split":
+        flags |= _cuda_impl.FLAG_SPLIT_DELAY
     if grid_shape is None:
         grid_shape = _grid.detect(scan_coords_m)
     options = _cuda_impl.make_options(

@@ -296,4 +296,25 @@ def to_storage(w: Workload, storage: str):
     raise ValueError(f"no conversion from {w.storage} to {storage}")
 
 
+def as_storage(w: Workload, storage: str):
+    """``(channel, channel_scale)`` of ``w`` in ``storage``; int16 storage is scaled to use
+    the range +-20000 (real RF keeps its own ADC scale when it already is int16)."""
+    import torch
+
+    if storage == w.storage:
+        return w.channel, w.channel_scale
+    if storage in ("ci16", "i16"):
+        x = w.channel
+        if x.dtype == torch.int16:
+            x = x.to(torch.float32) * w.channel_scale
+        x = torch.view_as_real(x.to(torch.complex64)) if storage == "ci16" else x.to(torch.float32)
+        scale = float(x.abs().max()) / 20000.0 or 1.0
+        return (x / scale).round().clamp(-32768, 32767).to(torch.int16).contiguous(), scale
+    ch = w.channel
+    if ch.dtype == torch.int16:
+        ch = ch.to(torch.float32) * w.channel_scale
+        w = Workload(w.name, ch, w.rx_coords_m, w.scan_coords_m, w.tx_wave_arrivals_s, w.params, "f32", 1.0)
+    return to_storage(w, storage), 1.0
+
+
 CONFIGS = {"plain2d": plain2d, "compound": compound, "doppler": doppler, "volume3d": volume3d}

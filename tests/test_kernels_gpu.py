@@ -88,3 +88,36 @@ def test_lane_voxel_storage(cuda, storage, n_frames):
     tuned = _run(w, tx_chunk=1)  # transmit-major summation order: FP32 rounding only
     assert H.rel_l2(got, tuned) <= 1e-5
     assert H.nrms_db(got, H.oracle(w, storage=storage)) <= -60.0
+
+
+@pytest.mark.parametrize("interp", [0, 1, 2])
+@pytest.mark.parametrize("kernel", ["lane_voxel", "staged"])
+def test_split_delay_is_more_accurate(cuda, interp, kernel):
+    """Split delays (FP64 per path, integer base + FP32 fraction) beat mach's FP32 delays
+    against the FP64 oracle, on both kernel families."""
+    w = H.small("compound") if kernel == "lane_voxel" else _workload("c64", 16, interp)
+    w.params["interp_type"] = interp
+    want = H.oracle(w)
+    ref_db = H.nrms_db(_run(w, kernel=kernel, delay="reference"), want)
+    split_db = H.nrms_db(_run(w, kernel=kernel, delay="split"), want)
+    print(f"{kernel} interp {interp}: reference delays {ref_db:.1f} dB, split delays {split_db:.1f} dB")
+    assert split_db <= ref_db + 0.5
+    assert split_db <= -75.0
+
+
+@pytest.mark.parametrize("storage", ["cf16", "ci16", "f16", "i16"])
+def test_split_delay_reduced_storage(cuda, storage):
+    w = _workload(storage, 16, 1)
+    got = _run(w)  # delay="auto" selects split delays for reduced storage
+    assert H.nrms_db(got, H.oracle(w, storage=storage)) <= -75.0
+
+
+@pytest.mark.parametrize("storage", STORAGES)
+@pytest.mark.parametrize("interp", [0, 1, 2])
+def test_lane_voxel_sixteen_frames(cuda, storage, interp):
+    """16-frame jobs take the vectorised voxel-per-lane path; it matches the other families."""
+    w = _workload(storage, 16, interp)
+    lane = _run(w, kernel="lane_voxel")
+    warp = _run(w, kernel="warp")
+    assert H.rel_l2(lane, warp) <= 2e-6
+    assert H.nrms_db(lane, H.oracle(w, storage=storage)) <= -60.0
