@@ -16,9 +16,10 @@
 //   c. the team's warps widen the rows to FP32 and store them into TMEM (tcgen05.st);
 //   d. each warp gathers its 32 voxels: one tcgen05.ld (both taps, both components) per
 //      voxel, then lerp, rotation and accumulation in FP32 registers.
-// Steps are pipelined (the window of step k+1 streams in while step k is gathered; TMEM
-// and the shared-memory window are double-buffered, parameters triple-buffered) with one
-// named barrier per team and step.  A step whose rows do not fit the window gathers
+// Steps are pipelined: parameters and the window copy run two steps ahead of the gather
+// (three shared-memory windows, four parameter slots, two TMEM windows), with one named
+// barrier per team and step.  Teams take items from a device counter, heaviest first
+// (deep tiles have the widest aperture), so the tail of a launch is made of light items.  A step whose rows do not fit the window gathers
 // straight from global memory.  All mbarrier waits are bounded; on a timeout the team
 // records an error in the status word and stops.  Every CTA frees its tensor memory
 // before it exits.
@@ -37,7 +38,11 @@ constexpr int kEnsTileVoxels = 128;                      // one voxel per team t
 constexpr int kEnsMaxPrefetchTx = 16;                    // arrivals of <= 16 transmits staged per item
 constexpr int kEnsMaxWindow = 64;
 
+constexpr int kEnsWindows = 3;  // shared-memory windows in flight
+constexpr int kEnsSlots = 4;    // parameter slots (steps k .. k + 2 plus one being read)
+
 struct EnsembleArgs {
+    int* counter;         // work-item counter, zero at launch
     int32_t window_rows;  // W: rows per window, a multiple of 16 in [16, 64]
     int32_t n_tiles;      // voxel tiles
     int32_t n_fblocks;    // frame blocks (32 lanes each)
@@ -119,24 +124,38 @@ __device__ __forceinline__ void tmem_st8(uint32_t col, const float2 (&v)[4]) {
                  "r"(__float_as_uint(v[3].x)), "r"(__float_as_uint(v[3].y))
                  : "memory");
 }
-// Two rows (linear taps) / one row (nearest) of this lane starting at column `col`.
-__device__ __forceinline__ void tmem_ld4(uint32_t col, uint32_t (&r)[4]) {
-    asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0, %1, %2, %3}, [%4];"
-                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
-                 : "r"(col));
+// Four loads of (row, row + 1) at columns c0..c3 and the wait for them, in one statement:
+// the outputs are only defined once tcgen05.wait::ld has retired the loads.
+__device__ __forceinline__ void tmem_ld4x4(const uint32_t (&c)[4], uint32_t (&r)[4][4]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0, %1, %2, %3}, [%16];\n\t"
+        "tcgen05.ld.sync.aligned.32x32b.x4.b32 {%4, %5, %6, %7}, [%17];\n\t"
+        "tcgen05.ld.sync.aligned.32x32b.x4.b32 {%8, %9, %10, %11}, [%18];\n\t"
+        "tcgen05.ld.sync.aligned.32x32b.x4.b32 {%12, %13, %14, %15}, [%19];\n\t"
+        "tcgen05.wait::ld.sync.aligned;"
+        : "=r"(r[0][0]), "=r"(r[0][1]), "=r"(r[0][2]), "=r"(r[0][3]), "=r"(r[1][0]), "=r"(r[1][1]), "=r"(r[1][2]),
+          "=r"(r[1][3]), "=r"(r[2][0]), "=r"(r[2][1]), "=r"(r[2][2]), "=r"(r[2][3]), "=r"(r[3][0]), "=r"(r[3][1]),
+          "=r"(r[3][2]), "=r"(r[3][3])
+        : "r"(c[0]), "r"(c[1]), "r"(c[2]), "r"(c[3])
+        : "memory");
 }
-__device__ __forceinline__ void tmem_ld2(uint32_t col, uint32_t (&r)[4]) {
-    asm volatile("tcgen05.ld.sync.aligned.32x32b.x2.b32 {%0, %1}, [%2];" : "=r"(r[0]), "=r"(r[1]) : "r"(col));
-    r[2] = r[0];
-    r[3] = r[1];
-}
-// Wait for this thread's tensor-memory loads; the register operands tie the loaded values
-// to the wait so no use is scheduled before it.
-template <int N>
-__device__ __forceinline__ void tmem_wait_ld(uint32_t (&r)[N][4]) {
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+// Same for one row (nearest taps); the second row of each result repeats the first.
+__device__ __forceinline__ void tmem_ld4x2(const uint32_t (&c)[4], uint32_t (&r)[4][4]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x2.b32 {%0, %1}, [%8];\n\t"
+        "tcgen05.ld.sync.aligned.32x32b.x2.b32 {%2, %3}, [%9];\n\t"
+        "tcgen05.ld.sync.aligned.32x32b.x2.b32 {%4, %5}, [%10];\n\t"
+        "tcgen05.ld.sync.aligned.32x32b.x2.b32 {%6, %7}, [%11];\n\t"
+        "tcgen05.wait::ld.sync.aligned;"
+        : "=r"(r[0][0]), "=r"(r[0][1]), "=r"(r[1][0]), "=r"(r[1][1]), "=r"(r[2][0]), "=r"(r[2][1]), "=r"(r[3][0]),
+          "=r"(r[3][1])
+        : "r"(c[0]), "r"(c[1]), "r"(c[2]), "r"(c[3])
+        : "memory");
 #pragma unroll
-    for (int i = 0; i < N; ++i) asm volatile("" : "+r"(r[i][0]), "+r"(r[i][1]), "+r"(r[i][2]), "+r"(r[i][3]));
+    for (int i = 0; i < 4; ++i) {
+        r[i][2] = r[i][0];
+        r[i][3] = r[i][1];
+    }
 }
 
 __device__ __forceinline__ void team_sync(int team) {
@@ -156,27 +175,29 @@ __device__ __forceinline__ bool team_sync_or(int team, bool flag) {
 // ------------------------------------------------------------------ shared memory per team
 
 struct EnsembleTeamSmem {
-    unsigned char* win;  // [2][W][32] lane words
-    StepParam* param;    // [3][128]
+    unsigned char* win;  // [kEnsWindows][W][32] lane words
+    StepParam* param;    // [kEnsSlots][128]
+    int2* lohi;          // [kEnsSlots][4] per-warp window partials (lo, hi)
+    unsigned* valid;     // [kEnsSlots][4] per-warp validity ballots
+    int* count;          // [4]
+    float* bbox;         // [4][5]
     float* arr;          // [n_pref][128]
     int64_t* vox;        // [128] voxel index of each tile slot (-1 outside the grid)
     int* cand;           // [128] candidate elements of the current element block
-    int* lohi;           // [3][4][2] per-warp window partials
-    unsigned* valid;     // [3][4] per-warp validity ballots
-    int* count;          // [4]
-    float* bbox;         // [4][5]
-    uint64_t* bar;       // [2]
+    int* item;           // [2] current work item
+    uint64_t* bar;       // [kEnsWindows]
 };
 
 __host__ __device__ inline int ensemble_team_bytes(int window_rows, int lane_word_bytes, int n_pref) {
-    int b = 2 * window_rows * 32 * lane_word_bytes;            // windows
-    b += 3 * kEnsTileVoxels * static_cast<int>(sizeof(StepParam));
+    int b = kEnsWindows * window_rows * 32 * lane_word_bytes;  // windows
+    b += kEnsSlots * kEnsTileVoxels * static_cast<int>(sizeof(StepParam));
+    b += (kEnsSlots * 4 * 2 + kEnsSlots * 4 + 4) * 4 + 4 * 5 * 4;  // partials, ballots, counts, bbox
     b += n_pref * kEnsTileVoxels * 4;                          // arrivals
     b += kEnsTileVoxels * 8;                                   // voxel indices
     b += kEnsTileVoxels * 4;                                   // candidates
-    b += (3 * 4 * 2 + 3 * 4 + 4) * 4 + 4 * 5 * 4;              // partials, ballots, counts, bbox
+    b += 2 * 4;                                                // work item
     b = (b + 7) & ~7;
-    b += 2 * 8;                                                // mbarriers
+    b += kEnsWindows * 8;                                      // mbarriers
     return (b + 127) & ~127;
 }
 
@@ -184,23 +205,25 @@ __device__ __forceinline__ EnsembleTeamSmem team_smem(unsigned char* base, int w
     EnsembleTeamSmem s;
     unsigned char* p = base;
     s.win = p;
-    p += 2 * window_rows * 32 * lwb;
+    p += kEnsWindows * window_rows * 32 * lwb;
     s.param = reinterpret_cast<StepParam*>(p);
-    p += 3 * kEnsTileVoxels * sizeof(StepParam);
+    p += kEnsSlots * kEnsTileVoxels * sizeof(StepParam);
+    s.lohi = reinterpret_cast<int2*>(p);  // 16-byte aligned: read as two int4 per slot
+    p += kEnsSlots * 4 * 2 * 4;
+    s.valid = reinterpret_cast<unsigned*>(p);
+    p += kEnsSlots * 4 * 4;
+    s.count = reinterpret_cast<int*>(p);
+    p += 4 * 4;
+    s.bbox = reinterpret_cast<float*>(p);
+    p += 4 * 5 * 4;
     s.arr = reinterpret_cast<float*>(p);
     p += n_pref * kEnsTileVoxels * 4;
     s.vox = reinterpret_cast<int64_t*>(p);
     p += kEnsTileVoxels * 8;
     s.cand = reinterpret_cast<int*>(p);
     p += kEnsTileVoxels * 4;
-    s.lohi = reinterpret_cast<int*>(p);
-    p += 3 * 4 * 2 * 4;
-    s.valid = reinterpret_cast<unsigned*>(p);
-    p += 3 * 4 * 4;
-    s.count = reinterpret_cast<int*>(p);
-    p += 4 * 4;
-    s.bbox = reinterpret_cast<float*>(p);
-    p += 4 * 5 * 4;
+    s.item = reinterpret_cast<int*>(p);
+    p += 2 * 4;
     p = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(p) + 7) & ~uintptr_t{7});
     s.bar = reinterpret_cast<uint64_t*>(p);
     return s;
@@ -235,8 +258,8 @@ __global__ void __launch_bounds__(kEnsThreads, 1)
     EnsembleTeamSmem s = team_smem(smem + team * ea.team_bytes, W, kLwb, n_pref);
 
     if (tt == 0) {
-        mbar_init(&s.bar[0], 1);
-        mbar_init(&s.bar[1], 1);
+#pragma unroll
+        for (int i = 0; i < kEnsWindows; ++i) mbar_init(&s.bar[i], 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 0) tmem_alloc(&s_tmem, ea.tmem_cols);
@@ -252,15 +275,24 @@ __global__ void __launch_bounds__(kEnsThreads, 1)
     uint32_t pending = 0u;  // bit b: a copy was issued on buffer b and has not been waited for
     bool dead = false;
 
-    for (int item = blockIdx.x * kEnsTeams + team; item < n_items && !dead; item += gridDim.x * kEnsTeams) {
-        const int tile = item % ea.n_tiles;
+    for (;;) {
+        team_sync(team);  // the previous item's shared state is consumed
+        if (tt == 0) s.item[0] = atomicAdd(ea.counter, 1);
+        team_sync(team);
+        const int item = s.item[0];
+        if (item >= n_items) break;
+        // Tiles in reverse order: for a scan ordered depth-fastest the deepest (widest
+        // aperture, most candidate elements) come first.
+        const int tile = ea.n_tiles - 1 - item % ea.n_tiles;
         const int fb = item / ea.n_tiles;
         const int64_t word0 = static_cast<int64_t>(fb) * 32 + lane;  // this lane's word within a row
         const bool lane_ok = word0 < row_words;
 
-        team_sync(team);  // the previous item's shared state is consumed
         // ---- this thread's voxel, its arrivals, the tile bounding box
-        const int64_t pv = tile_voxel(a, st, tile, tt);
+        // Team thread (tw, lane) owns tile slot 4 * (4 * (lane >> 2) + tw) + (lane & 3): each warp
+        // holds every fourth column of 4-voxel runs along the contiguous axis, so the four
+        // warps see similar apertures and finish their gathers together.
+        const int64_t pv = tile_voxel(a, st, tile, 4 * (4 * (lane >> 2) + tw) + (lane & 3));
         s.vox[tt] = pv;
         float vx = 0.f, vy = 0.f, vz = 0.f;
         if (pv >= 0) {
@@ -366,7 +398,7 @@ __global__ void __launch_bounds__(kEnsThreads, 1)
                     pair_ok = pv >= 0 && !(h2 > radius_sq) && !(weight == 0.0f);
                     weight_scaled = __fmul_rn(weight, a.scale);
                 }
-                StepParam p{-(1 << 30), 0.f, 0.f, 0.f};
+                StepParam p{-(1 << 28), 0.f, 0.f, 0.f};
                 int lo = 0x7fffffff, hi = -1;
                 bool ok = false;
                 if (pair_ok) {
@@ -419,20 +451,17 @@ __global__ void __launch_bounds__(kEnsThreads, 1)
                 lo = __reduce_min_sync(kFull, lo);
                 hi = __reduce_max_sync(kFull, hi);
                 if (lane == 0) {
-                    s.lohi[(slot * 4 + tw) * 2 + 0] = lo;
-                    s.lohi[(slot * 4 + tw) * 2 + 1] = hi;
+                    s.lohi[slot * 4 + tw] = make_int2(lo, hi);
                     s.valid[slot * 4 + tw] = vmask;
                 }
             };
             // ---- after the team barrier: step k's window and mode (every thread), copy start (thread 0)
             int w_ci = 0, w_t = 0;  // step cursor of the window phase
             auto plan_window = [&](int slot, int b, int& lo_out) -> int {
-                int lo = 0x7fffffff, hi = -1;
-#pragma unroll
-                for (int w = 0; w < 4; ++w) {
-                    lo = min(lo, s.lohi[(slot * 4 + w) * 2 + 0]);
-                    hi = max(hi, s.lohi[(slot * 4 + w) * 2 + 1]);
-                }
+                const int4 q0 = reinterpret_cast<const int4*>(s.lohi + slot * 4)[0];
+                const int4 q1 = reinterpret_cast<const int4*>(s.lohi + slot * 4)[1];
+                const int lo = min(min(q0.x, q0.z), min(q1.x, q1.z));
+                const int hi = max(max(q0.y, q0.w), max(q1.y, q1.w));
                 const int e = s.cand[w_ci];
                 const int t = w_t;
                 if (++w_t == a.n_tx) {
@@ -451,21 +480,32 @@ __global__ void __launch_bounds__(kEnsThreads, 1)
                 return mode;
             };
 
+            // Planned steps k and k + 1: window start, mode, element, transmit.
+            int q_lo[2] = {0, 0}, q_mode[2] = {kEnsModeEmpty, kEnsModeEmpty}, q_e[2] = {0, 0}, q_t[2] = {0, 0};
             make_params(0);
+            if (n_steps > 1) make_params(1);
             tmem_fence_before();
             team_sync(team);
             tmem_fence_after();
-            int cur_lo, cur_mode, cur_e, cur_t;
-            cur_e = s.cand[0];
-            cur_t = 0;
-            cur_mode = plan_window(0, 0, cur_lo);
+            q_e[0] = s.cand[w_ci];
+            q_t[0] = w_t;
+            q_mode[0] = plan_window(0, 0, q_lo[0]);
+            if (n_steps > 1) {
+                q_e[1] = s.cand[w_ci];
+                q_t[1] = w_t;
+                q_mode[1] = plan_window(1, 1, q_lo[1]);
+            }
 
+            int wb = 0;  // shared-memory window of step k (k % 3)
             for (int k = 0; k < n_steps; ++k) {
-                const int slot = k % 3;
-                const int b = k & 1;
-                if (k + 1 < n_steps) make_params((k + 1) % 3);
+                const int slot = k & (kEnsSlots - 1);
+                const int tb = k & 1;  // TMEM window of step k
+                const int wb2 = wb == 0 ? 2 : wb - 1;  // window of step k + 2
+                const int cur_lo = q_lo[0], cur_mode = q_mode[0], cur_e = q_e[0], cur_t = q_t[0];
+                if (k + 2 < n_steps) make_params((k + 2) & (kEnsSlots - 1));
                 // ---- window k: wait for its copy, widen its rows into TMEM (this warp's quarter)
                 bool timed_out = false;
+                const int b = wb;
                 if (cur_mode == kEnsModeWindow) {
                     if (mbar_wait(&s.bar[b], (phase >> b) & 1u)) {
                         phase ^= 1u << b;
@@ -479,7 +519,7 @@ __global__ void __launch_bounds__(kEnsThreads, 1)
                         const int rows = W >> 2;
                         const int r0 = tw * rows;
                         const Word* src = reinterpret_cast<const Word*>(s.win + b * W * 32 * kLwb) + lane;
-                        const uint32_t col0 = tbase + static_cast<uint32_t>(b * 2 * W);
+                        const uint32_t col0 = tbase + static_cast<uint32_t>(tb * 2 * W);
                         for (int r = r0; r < r0 + rows; r += 4) {
                             float2 v[4];
 #pragma unroll
@@ -495,34 +535,34 @@ __global__ void __launch_bounds__(kEnsThreads, 1)
                     break;
                 }
                 tmem_fence_after();
-                // ---- start the copy of step k + 1
-                int next_lo = 0, next_mode = kEnsModeEmpty, next_e = 0, next_t = 0;
-                if (k + 1 < n_steps) {
-                    next_e = s.cand[w_ci];
-                    next_t = w_t;
-                    next_mode = plan_window((k + 1) % 3, b ^ 1, next_lo);
+                // ---- start the copy of step k + 2
+                int n_lo = 0, n_mode = kEnsModeEmpty, n_e = 0, n_t = 0;
+                if (k + 2 < n_steps) {
+                    n_e = s.cand[w_ci];
+                    n_t = w_t;
+                    n_mode = plan_window((k + 2) & (kEnsSlots - 1), wb2, n_lo);
                 }
                 // ---- gather step k
                 const unsigned vm = s.valid[slot * 4 + tw];
                 const StepParam* prm = s.param + slot * kEnsTileVoxels + tw * 32;
                 if (cur_mode == kEnsModeWindow && vm != 0u) {
-                    const uint32_t colb = tbase + static_cast<uint32_t>(b * 2 * W);
+                    const int colb = static_cast<int>(tbase) + tb * 2 * W;  // column of row lo
+                    const int cb = colb - 2 * cur_lo;
 #pragma unroll
                     for (int g = 0; g < 8; ++g) {
                         if (((vm >> (4 * g)) & 0xfu) == 0u) continue;
                         StepParam p[4];
-                        uint32_t r[4][4];
+                        uint32_t r[4][4], col[4];
 #pragma unroll
                         for (int i = 0; i < 4; ++i) {
                             p[i] = prm[4 * g + i];
-                            const uint32_t col = colb + 2u * static_cast<uint32_t>(max(p[i].row - cur_lo, 0));
-                            if constexpr (INTERP == kLinear) {
-                                tmem_ld4(col, r[i]);
-                            } else {
-                                tmem_ld2(col, r[i]);
-                            }
+                            col[i] = static_cast<uint32_t>(max(2 * p[i].row + cb, colb));
                         }
-                        tmem_wait_ld(r);
+                        if constexpr (INTERP == kLinear) {
+                            tmem_ld4x4(col, r);
+                        } else {
+                            tmem_ld4x2(col, r);
+                        }
 #pragma unroll
                         for (int i = 0; i < 4; ++i) {
                             const float ax = __uint_as_float(r[i][0]), ay = __uint_as_float(r[i][1]);
@@ -570,10 +610,15 @@ __global__ void __launch_bounds__(kEnsThreads, 1)
                         }
                     }
                 }
-                cur_lo = next_lo;
-                cur_mode = next_mode;
-                cur_e = next_e;
-                cur_t = next_t;
+                q_lo[0] = q_lo[1];
+                q_mode[0] = q_mode[1];
+                q_e[0] = q_e[1];
+                q_t[0] = q_t[1];
+                q_lo[1] = n_lo;
+                q_mode[1] = n_mode;
+                q_e[1] = n_e;
+                q_t[1] = n_t;
+                wb = wb == 2 ? 0 : wb + 1;
             }
         }
         if (dead) break;
@@ -608,8 +653,10 @@ __global__ void __launch_bounds__(kEnsThreads, 1)
 
     if (dead) {
         // Give copies still in flight a bounded chance to land before the CTA exits.
-        if (pending & 1u) mbar_wait(&s.bar[0], phase & 1u);
-        if (pending & 2u) mbar_wait(&s.bar[1], (phase >> 1) & 1u);
+#pragma unroll
+        for (int i = 0; i < kEnsWindows; ++i) {
+            if ((pending >> i) & 1u) mbar_wait(&s.bar[i], (phase >> i) & 1u);
+        }
         if (tt == 0) atomicOr(st.status, 1);
     }
     tmem_fence_before();

@@ -191,7 +191,7 @@ __device__ __forceinline__ int64_t tile_voxel(const DasArgs& a, const StagedArgs
 }
 
 // Per-voxel step parameters in shared memory (16 bytes, one broadcast load per round).
-struct StepParam {
+struct alignas(16) StepParam {
     int row;   // tap row (TMA mode: absolute sample index, the window start is subtracted later)
     float w;   // linear: fraction t; quadratic: offset x from the centre tap; nearest: unused
     float cw;  // weight x cos(phase) (real data: the weight)

@@ -234,9 +234,13 @@ bool plan_ensemble(int storage, int interp, uint64_t n_vox, uint32_t n_frames, u
         ea.n_tiles = static_cast<int32_t>((n_vox + kEnsTileVoxels - 1) / kEnsTileVoxels);
     }
     if (static_cast<int64_t>(ea.n_tiles) * ea.n_fblocks > 0x7fffffffll) return false;
+    const int n_pref = n_tx <= static_cast<uint32_t>(kEnsMaxPrefetchTx) ? static_cast<int>(n_tx) : 0;
+    // Four teams' buffers must fit the 227 KB a CTA may use.
+    while (w > 16 && kEnsTeams * ensemble_team_bytes(w, lwb, n_pref) > 227 * 1024) w -= 16;
+    ea.window_rows = w;
+    ea.tmem_cols = static_cast<uint32_t>(std::max(32, next_pow2(4 * w)));
     st.use_tma = 1;
     st.window_rows = w;
-    const int n_pref = n_tx <= static_cast<uint32_t>(kEnsMaxPrefetchTx) ? static_cast<int>(n_tx) : 0;
     ea.team_bytes = ensemble_team_bytes(w, lwb, n_pref);
     p.ensemble = true;
     p.staged = false;
@@ -403,6 +407,22 @@ cudaError_t dispatch(int storage, const DasArgs& a, int interp, const Plan& plan
 #undef MACH_B200_CASE
 }
 
+// Stream-ordered device buffer released at scope exit (on the stream it was allocated on).
+struct DeviceBuffer {
+    void* ptr = nullptr;
+    cudaStream_t stream = nullptr;
+    DeviceBuffer() = default;
+    DeviceBuffer(const DeviceBuffer&) = delete;
+    DeviceBuffer& operator=(const DeviceBuffer&) = delete;
+    cudaError_t alloc(size_t bytes, cudaStream_t st) {
+        stream = st;
+        return cudaMallocAsync(&ptr, bytes ? bytes : 1, st);
+    }
+    ~DeviceBuffer() {
+        if (ptr) cudaFreeAsync(ptr, stream);
+    }
+};
+
 // Launch transmits [0, a.n_tx) so that every launch's channel span stays below 2^31 samples
 // (32-bit offsets inside the kernels).  Later launches always accumulate.
 int dispatch_split(int storage, DasArgs a, int interp, const Plan& plan, cudaStream_t st) {
@@ -412,6 +432,15 @@ int dispatch_split(int storage, DasArgs a, int interp, const Plan& plan, cudaStr
     const char* ch = static_cast<const char*>(a.channel);
     const float* arr = a.arrivals;
     const int total = a.n_tx;
+    // Ensemble launches take work items from a zeroed device counter (one per launch).
+    const int n_launch = static_cast<int>((std::max(total, 1) + max_tx - 1) / max_tx);
+    DeviceBuffer counters;
+    Plan pl = plan;
+    if (plan.ensemble) {
+        MACH_B200_CUDA_TRY(counters.alloc(sizeof(int) * n_launch, st));
+        MACH_B200_CUDA_TRY(cudaMemsetAsync(counters.ptr, 0, sizeof(int) * n_launch, st));
+    }
+    int launch = 0;
     int t0 = 0;
     do {
         DasArgs b = a;
@@ -428,27 +457,13 @@ int dispatch_split(int storage, DasArgs a, int interp, const Plan& plan, cudaStr
                                               plan.st.window_rows);
             if (rc) return rc;
         }
-        MACH_B200_CUDA_TRY(dispatch(storage, b, interp, plan, map, st));
+        if (plan.ensemble) pl.ea.counter = static_cast<int*>(counters.ptr) + launch;
+        MACH_B200_CUDA_TRY(dispatch(storage, b, interp, pl, map, st));
+        ++launch;
         t0 += static_cast<int>(max_tx);
     } while (t0 < total);
     return MACH_B200_OK;
 }
-
-// Stream-ordered device buffer released at scope exit (on the stream it was allocated on).
-struct DeviceBuffer {
-    void* ptr = nullptr;
-    cudaStream_t stream = nullptr;
-    DeviceBuffer() = default;
-    DeviceBuffer(const DeviceBuffer&) = delete;
-    DeviceBuffer& operator=(const DeviceBuffer&) = delete;
-    cudaError_t alloc(size_t bytes, cudaStream_t st) {
-        stream = st;
-        return cudaMallocAsync(&ptr, bytes ? bytes : 1, st);
-    }
-    ~DeviceBuffer() {
-        if (ptr) cudaFreeAsync(ptr, stream);
-    }
-};
 
 struct EventPair {
     cudaEvent_t ev[2] = {nullptr, nullptr};
