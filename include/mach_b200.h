@@ -145,6 +145,36 @@ MACH_B200_API int mach_b200_beamform_ex(int32_t storage, const void* channel_dat
                                 int32_t interp_type, float channel_scale, void* cuda_stream,
                                 const mach_b200_options* options);
 
+/*
+ * mach_b200_beamform_ex restricted to the ensemble kernel (MACH_B200_KERNEL_ENSEMBLE), for
+ * callers that must not allocate GPU memory: a host that pre-reserves all of HBM for its own
+ * allocator, or a real-time acquisition loop that cannot risk a pool growing (and stalling)
+ * inside a call.  The ensemble kernel's only scratch, one work-item counter per launch, lives
+ * in a static device array of the library (64 counters, 256 bytes on every device that loads
+ * it) instead of a stream-ordered allocation; the call allocates, copies and frees nothing.
+ * No counterpart in the reference (mach allocates staging buffers and runs one fixed kernel).
+ *
+ * - Every buffer must be device memory of the current device.  The job must fit the ensemble
+ *   kernel (nearest or linear interpolation, 16-byte aligned channel_data, n_frames x sample
+ *   bytes a multiple of 16, fewer than 2^31 voxels) and need at most 64 launches, i.e. at most
+ *   64 x (2^31 - 1) channel samples; anything else is rejected with MACH_B200_ERR_VALUE.
+ * - The first call on a device looks up the counters' device address; make that first call
+ *   before any stream capture.
+ * - All calls share the counters (each call zeroes the ones it uses on `cuda_stream`), so two
+ *   calls whose work overlaps on the GPU (different streams, or MACH_B200_FLAG_ASYNC calls not
+ *   yet finished on other streams) race and give wrong images.  Serialise them.
+ * - Same arguments, flags and result as mach_b200_beamform_ex.
+ */
+MACH_B200_API int mach_b200_beamform_ensemble_noalloc(int32_t storage, const void* channel_data,
+                                const float* rx_coords_m, const float* scan_coords_m,
+                                const float* tx_wave_arrivals_s, void* out, uint32_t n_tx,
+                                uint32_t n_rx, uint32_t n_samples, uint64_t n_scan,
+                                uint32_t n_frames, float f_number, float rx_start_s,
+                                float sampling_freq_hz, float sound_speed_m_s,
+                                float modulation_freq_hz, float tukey_alpha,
+                                int32_t interp_type, float channel_scale, void* cuda_stream,
+                                const mach_b200_options* options);
+
 /* One job of a batch: every pointer must be device memory of the current device. */
 typedef struct mach_b200_job {
     int32_t storage;             /* MACH_B200_STORAGE_* */

@@ -41,6 +41,12 @@ MACH_B200_EXTERN(kCI16)
 // Status word written by kernels whose bounded waits time out (one per device).
 __device__ int g_mach_b200_status;
 
+// Work-item counters of mach_b200_beamform_ensemble_noalloc: one per launch (a launch covers
+// fewer than 2^31 channel samples), kNoAllocLaunches at most: 256 bytes held on every device
+// that loads the library.  Every call shares them; each call zeroes the ones it uses.
+constexpr int kNoAllocLaunches = 64;
+static __device__ __align__(256) int g_noalloc_counters[kNoAllocLaunches];
+
 namespace {
 
 using namespace mach_b200;
@@ -728,6 +734,129 @@ mach_b200_options default_options(uint32_t flags) {
 }
 
 
+// ---------------------------------------------------------------- allocation-free ensemble call
+//
+// mach_b200_beamform_ensemble_noalloc runs the ensemble kernel without allocating anything.
+// The kernel's only scratch is one work-item counter per launch; here those counters live
+// in this file's static device array instead of a stream-ordered allocation.
+
+struct NoAllocState {
+    std::once_flag once;
+    cudaError_t init_error = cudaSuccess;
+    int* counters = nullptr;  // device address of g_noalloc_counters
+};
+NoAllocState g_noalloc[kMaxDevices];
+
+// First call on a device (that device current): the device address of the counters.  In host
+// code g_noalloc_counters names a host-side stand-in, never the device memory itself.
+int noalloc_counters(int device, int** out) {
+    if (device < 0 || device >= kMaxDevices) return fail(MACH_B200_ERR_DEVICE, "device %d out of range", device);
+    NoAllocState& d = g_noalloc[device];
+    std::call_once(d.once, [&d]() {
+        void* p = nullptr;
+        d.init_error = cudaGetSymbolAddress(&p, g_noalloc_counters);
+        d.counters = static_cast<int*>(p);
+    });
+    if (d.init_error != cudaSuccess) {
+        return fail(MACH_B200_ERR_CUDA, "scratch setup failed: %s", cudaGetErrorString(d.init_error));
+    }
+    *out = d.counters;
+    return MACH_B200_OK;
+}
+
+int noalloc_impl(int32_t storage, const void* channel_data, const float* rx_coords_m, const float* scan_coords_m,
+                 const float* tx_wave_arrivals_s, void* out, uint32_t n_tx, uint32_t n_rx, uint32_t n_samples,
+                 uint64_t n_scan, uint32_t n_frames, float f_number, float rx_start_s, float sampling_freq_hz,
+                 float sound_speed_m_s, float modulation_freq_hz, float tukey_alpha, int32_t interp_type,
+                 float channel_scale, cudaStream_t stream, const mach_b200_options& opt) {
+    g_error.clear();
+    const uint32_t flags = opt.flags;
+    int rc = check_args(storage, interp_type, tukey_alpha, n_tx, n_rx, n_samples, n_scan, n_frames);
+    if (rc) return rc;
+    if (n_scan == 0 || n_frames == 0) return MACH_B200_OK;
+    if (!out || !scan_coords_m) return fail(MACH_B200_ERR_VALUE, "out and scan_coords_m must not be NULL");
+    const bool need_channel = n_tx > 0 && n_rx > 0 && n_samples > 0;
+    if (need_channel && (!channel_data || !rx_coords_m || !tx_wave_arrivals_s)) {
+        return fail(MACH_B200_ERR_VALUE, "channel_data, rx_coords_m and tx_wave_arrivals_s must not be NULL");
+    }
+    int device = 0;
+    MACH_B200_CUDA_TRY(cudaGetDevice(&device));
+    DeviceState* dev = nullptr;
+    if ((rc = device_state(device, &dev))) return rc;
+    int* counters = nullptr;
+    if ((rc = noalloc_counters(device, &counters))) return rc;
+    const void* ptrs[5] = {channel_data, rx_coords_m, scan_coords_m, tx_wave_arrivals_s, out};
+    const char* names[5] = {"channel_data", "rx_coords_m", "scan_coords_m", "tx_wave_arrivals_s", "out"};
+    for (int i = 0; i < 5; ++i) {
+        if (!ptrs[i]) continue;  // only optional inputs can be NULL here (checked above)
+        Residency r;
+        if ((rc = residency(ptrs[i], device, &r, names[i]))) return rc;
+        if (r != kOnDevice) {
+            return fail(MACH_B200_ERR_VALUE, "%s must be device memory: this call copies and allocates nothing",
+                        names[i]);
+        }
+    }
+    Plan plan;
+    if (!plan_ensemble(storage, interp_type, n_scan, n_frames, n_tx, channel_data, true, opt, plan)) {
+        return fail(MACH_B200_ERR_VALUE,
+                    "this job does not fit the ensemble kernel: it needs nearest or linear interpolation, a "
+                    "16-byte aligned channel_data, n_frames x sample bytes a multiple of 16 and fewer than 2^31 "
+                    "voxels");
+    }
+    plan.st.status = dev->status;
+    const bool cplx = (storage & 1) != 0;
+    DasArgs a = make_args(rx_coords_m, scan_coords_m, n_scan, need_channel ? n_rx : 0, n_samples, n_frames, f_number,
+                          rx_start_s, sampling_freq_hz, sound_speed_m_s, modulation_freq_hz, tukey_alpha,
+                          channel_scale, cplx, flags);
+    a.frame_passes = plan.lp.passes;
+    a.tx_chunk = plan.lp.tx_chunk;
+    a.channel = channel_data;
+    a.arrivals = tx_wave_arrivals_s;
+    a.out = out;
+    a.n_tx = static_cast<int32_t>(need_channel ? n_tx : 0);
+    a.accumulate = (flags & MACH_B200_FLAG_OVERWRITE) ? 0 : 1;
+
+    // Launches of fewer than 2^31 channel samples each, one counter per launch.
+    const size_t esz = storage_bytes(storage);
+    const int64_t per_tx = static_cast<int64_t>(a.n_rx) * a.row_stride;
+    const int64_t max_tx = std::max<int64_t>(1, ((int64_t{1} << 31) - 1) / std::max<int64_t>(per_tx, 1));
+    const int total = a.n_tx;
+    const int64_t n_launch = (std::max(total, 1) + max_tx - 1) / max_tx;
+    if (n_launch > kNoAllocLaunches) {
+        return fail(MACH_B200_ERR_VALUE,
+                    "this job needs %lld launches; the allocation-free call holds work counters for %d (at most "
+                    "%d x (2^31 - 1) channel samples)",
+                    static_cast<long long>(n_launch), kNoAllocLaunches, kNoAllocLaunches);
+    }
+    MACH_B200_CUDA_TRY(cudaMemsetAsync(counters, 0, sizeof(int) * static_cast<size_t>(n_launch), stream));
+    const char* ch = static_cast<const char*>(a.channel);
+    Plan pl = plan;
+    int t0 = 0;
+    for (int64_t launch = 0; launch < n_launch; ++launch) {
+        DasArgs b = a;
+        b.n_tx = static_cast<int32_t>(std::min<int64_t>(max_tx, total - t0));
+        b.channel = ch + static_cast<size_t>(t0) * per_tx * esz;
+        b.arrivals = a.arrivals + static_cast<int64_t>(t0) * a.n_vox;
+        b.accumulate = t0 == 0 ? a.accumulate : 1;
+        CUtensorMap map;
+        std::memset(&map, 0, sizeof(map));
+        if (b.n_tx > 0) {
+            if ((rc = encode_channel_map(&map, storage, b.channel, static_cast<uint64_t>(b.n_tx) * a.n_rx * a.n_samples,
+                                         a.n_frames, plan.ea.box_x, plan.st.window_rows))) {
+                return rc;
+            }
+        }
+        pl.ea.counter = counters + launch;
+        MACH_B200_CUDA_TRY(dispatch(storage, b, interp_type, pl, map, stream));
+        t0 += static_cast<int>(max_tx);
+    }
+    if (!(flags & MACH_B200_FLAG_ASYNC)) {
+        MACH_B200_CUDA_TRY(cudaStreamSynchronize(stream));
+        return check_status(dev, stream);
+    }
+    return MACH_B200_OK;
+}
+
 // ---------------------------------------------------------------- batches
 
 }  // namespace
@@ -1023,6 +1152,27 @@ int mach_b200_beamform_ex(int32_t storage, const void* channel_data, const float
                          n_samples, n_scan, n_frames, f_number, rx_start_s, sampling_freq_hz, sound_speed_m_s,
                          modulation_freq_hz, tukey_alpha, interp_type, channel_scale,
                          static_cast<cudaStream_t>(cuda_stream), o);
+}
+
+int mach_b200_beamform_ensemble_noalloc(int32_t storage, const void* channel_data, const float* rx_coords_m,
+                                        const float* scan_coords_m, const float* tx_wave_arrivals_s, void* out,
+                                        uint32_t n_tx, uint32_t n_rx, uint32_t n_samples, uint64_t n_scan,
+                                        uint32_t n_frames, float f_number, float rx_start_s, float sampling_freq_hz,
+                                        float sound_speed_m_s, float modulation_freq_hz, float tukey_alpha,
+                                        int32_t interp_type, float channel_scale, void* cuda_stream,
+                                        const mach_b200_options* options) {
+    mach_b200_options o = default_options(0u);
+    if (options) {
+        if (options->struct_size < offsetof(mach_b200_options, reserved)) {
+            g_error = "mach_b200_options.struct_size is too small";
+            return MACH_B200_ERR_VALUE;
+        }
+        std::memcpy(&o, options, std::min<size_t>(sizeof(o), options->struct_size));
+    }
+    return noalloc_impl(storage, channel_data, rx_coords_m, scan_coords_m, tx_wave_arrivals_s, out, n_tx, n_rx,
+                        n_samples, n_scan, n_frames, f_number, rx_start_s, sampling_freq_hz, sound_speed_m_s,
+                        modulation_freq_hz, tukey_alpha, interp_type, channel_scale,
+                        static_cast<cudaStream_t>(cuda_stream), o);
 }
 
 int mach_b200_batch_create(uint32_t max_jobs, mach_b200_batch** batch) { return batch_create(max_jobs, batch); }
