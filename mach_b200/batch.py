@@ -180,18 +180,25 @@ class Batch:
         arr = self._structs()
         _cuda_impl._raise_for(_lib.mach_b200_batch_run(self._handle, arr, len(self.jobs), stream.cuda_stream, flags))
 
-    def capture(self) -> None:
-        """Record the batch once in a CUDA graph (jobs and buffers fixed from now on)."""
+    def capture(self, warmup: bool = True) -> None:
+        """Record the batch once in a CUDA graph (jobs and buffers fixed from now on).
+
+        ``warmup`` first runs the batch synchronously, so lazy module loading happens
+        outside the capture; a batch that has already run once can skip it.  Capturing
+        only records: nothing runs until :meth:`replay`.
+        """
         import torch
 
-        self.run(sync=True)  # warm up: lazy module loading and the occupancy queries happen outside capture
+        if warmup:
+            self.run(sync=True)
         side = torch.cuda.Stream()
-        side.wait_stream(torch.cuda.current_stream())
         graph = torch.cuda.CUDAGraph()
         with torch.cuda.stream(side):
-            with torch.cuda.graph(graph, stream=side, capture_error_mode="relaxed"):
+            graph.capture_begin(capture_error_mode="relaxed")
+            try:
                 self.run(sync=False, stream=side)
-        torch.cuda.current_stream().wait_stream(side)
+            finally:
+                graph.capture_end()
         self._graph = graph
 
     def replay(self) -> None:
