@@ -454,12 +454,12 @@ def run_serving(args, world, rank, local):
     clocks.start()
     launches0 = _cuda_impl.launch_count()
     replayed0 = engine.executor.replayed_kernels
+    captured0 = engine.executor.captured_kernels
     waves0 = len(engine.scheduler.waves)
     hits0 = engine.executor.graph_hits
     engine.serve(reqs)
-    # (a graph capture records launches through the library without running them; captures
-    # are rare after warm-up and are counted as launches here)
-    launches = (_cuda_impl.launch_count() - launches0) + (engine.executor.replayed_kernels - replayed0)
+    launches = ((_cuda_impl.launch_count() - launches0) + (engine.executor.replayed_kernels - replayed0)
+                - (engine.executor.captured_kernels - captured0))
     clock_info = clocks.stop()
     makespan = max_over_ranks(max(r.done_s for r in reqs), world)
     points = sum(classes[r.cls].points for r in reqs)

@@ -238,6 +238,7 @@ class GpuExecutor:
         self.graph_hits = 0
         self.graph_misses = 0
         self.replayed_kernels = 0  # kernels launched by graph replays (the library counts direct launches)
+        self.captured_kernels = 0  # launches the library counted while recording graphs (never run)
         self.t0_event = None
         self.t0 = 0.0
 
@@ -279,6 +280,7 @@ class GpuExecutor:
                 batch.kernels = _cuda_impl.launch_count() - before
                 if self.use_graphs:
                     batch.capture(warmup=False)
+                    self.captured_kernels += batch.kernels
                     self.graphs[key] = batch
             done = torch.cuda.Event(enable_timing=True)
             done.record(stream)
