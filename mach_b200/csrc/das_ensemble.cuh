@@ -516,15 +516,20 @@ __global__ void __launch_bounds__(kEnsThreads, 1)
                     // tcgen05.st is warp-collective: the whole warp copies or none of it does.
                     timed_out = __any_sync(kFull, timed_out);
                     if (!timed_out) {
+                        // This warp's quarter of the rows, four rows (one 8-column store) at a time;
+                        // W / 4 is a multiple of 4 and at most 16.
                         const int rows = W >> 2;
                         const int r0 = tw * rows;
-                        const Word* src = reinterpret_cast<const Word*>(s.win + b * W * 32 * kLwb) + lane;
-                        const uint32_t col0 = tbase + static_cast<uint32_t>(tb * 2 * W);
-                        for (int r = r0; r < r0 + rows; r += 4) {
-                            float2 v[4];
+                        const Word* src = reinterpret_cast<const Word*>(s.win + b * W * 32 * kLwb) + r0 * 32 + lane;
+                        const uint32_t col0 = tbase + static_cast<uint32_t>(tb * 2 * W + 2 * r0);
 #pragma unroll
-                            for (int q = 0; q < 4; ++q) v[q] = LW::widen(src[(r + q) * 32]);
-                            tmem_st8(col0 + static_cast<uint32_t>(2 * r), v);
+                        for (int j = 0; j < kEnsMaxWindow / 16; ++j) {
+                            if (4 * j < rows) {
+                                float2 v[4];
+#pragma unroll
+                                for (int q = 0; q < 4; ++q) v[q] = LW::widen(src[(4 * j + q) * 32]);
+                                tmem_st8(col0 + static_cast<uint32_t>(8 * j), v);
+                            }
                         }
                         tmem_wait_st();
                     }
