@@ -62,6 +62,10 @@ extern "C" {
 #define MACH_B200_FLAG_SPLIT_DELAY 4u /* sample positions and phases formed in FP64 per receive path and
                                          per transmit, combined as integer base + FP32 fraction (more
                                          accurate than mach's FP32 delay; not bit-identical to mach) */
+#define MACH_B200_FLAG_POWER_DOPPLER 8u /* out is float32 [n_scan]: the power-Doppler image, the sum over
+                                           frames of |beamformed value|^2 (the step after the beamformer
+                                           in mach's examples/doppler.py:252), fused into the kernel where
+                                           it can be; only the compound / _ex entry points take it */
 
 /* Kernel families (mach_b200_options.kernel). */
 #define MACH_B200_KERNEL_AUTO 0

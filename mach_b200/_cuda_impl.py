@@ -92,6 +92,7 @@ library_path: str = str(_LIB_PATH)
 FLAG_ASYNC = 1
 FLAG_OVERWRITE = 2
 FLAG_SPLIT_DELAY = 4
+FLAG_POWER_DOPPLER = 8
 
 STORAGE_CODES = {"f32": 0, "c64": 1, "f16": 2, "cf16": 3, "bf16": 4, "cbf16": 5, "i16": 6, "ci16": 7}
 

@@ -129,6 +129,7 @@ struct DasArgs {
     // Split-delay mode: sample positions and phases formed in FP64 per (voxel, element) and
     // per (voxel, transmit), each split into an integer sample base + FP32 fraction.
     int32_t split;
+    int32_t power;          // ensemble kernel: out is float [n_vox], += sum over frames of |x|^2
     int32_t start_base;     // floor(-t0 * fs): samples before it belong to tau < 0
     float start_frac;       // -t0 * fs - start_base
     double fs_d;            // sampling frequency

@@ -628,6 +628,21 @@ __global__ void __launch_bounds__(kEnsThreads, 1)
         }
         if (dead) break;
 
+        // ---- power-Doppler epilogue: |x|^2 summed over this frame block (the warp's lanes),
+        // one atomic add per voxel (frame blocks of a voxel add in any order)
+        if (a.power) {
+            float mine = 0.f;
+#pragma unroll
+            for (int i = 0; i < 32; ++i) {
+                float pw = lane_ok ? __fmaf_rn(acc[i].x, acc[i].x, __fmul_rn(acc[i].y, acc[i].y)) : 0.f;
+#pragma unroll
+                for (int off = 16; off > 0; off >>= 1) pw += __shfl_xor_sync(kFull, pw, off);
+                if (lane == i) mine = pw;
+            }
+            const int64_t v = s.vox[tw * 32 + lane];
+            if (v >= 0) atomicAdd(static_cast<float*>(a.out) + v, mine);
+            continue;
+        }
         // ---- write this item's sums: lane word `word0` of each of this warp's 32 voxels
         if (lane_ok) {
 #pragma unroll

@@ -168,6 +168,10 @@ cudaError_t launch_staged_persistent(int interp, int lanes, const PersistentLaun
 #undef MACH_B200_PST
 }
 
+// Power-Doppler epilogue (das_power.cu): out[v] (+)= sum over frames of |in[v][f]|^2.
+cudaError_t launch_power_epilogue(const void* in, float* out, int64_t n_vox, int n_frames, bool cplx, bool accumulate,
+                                  cudaStream_t stream);
+
 // Ensemble kernel: persistent grid of at most one CTA per SM (its 512 threads use the whole
 // register file), each CTA running four teams over the (tile, frame block) items.
 template <int S, int I, bool SPLIT>

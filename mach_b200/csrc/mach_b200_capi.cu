@@ -574,11 +574,22 @@ int check_args(int32_t storage, int32_t interp_type, float tukey_alpha, uint32_t
     return MACH_B200_OK;
 }
 
+int power_impl(int32_t storage, const void* channel_data, const float* rx_coords_m, const float* scan_coords_m,
+               const float* tx_wave_arrivals_s, void* out, uint32_t n_tx, uint32_t n_rx, uint32_t n_samples,
+               uint64_t n_scan, uint32_t n_frames, float f_number, float rx_start_s, float sampling_freq_hz,
+               float sound_speed_m_s, float modulation_freq_hz, float tukey_alpha, int32_t interp_type,
+               float channel_scale, cudaStream_t stream, const mach_b200_options& opt);
+
 int compound_impl(int32_t storage, const void* channel_data, const float* rx_coords_m, const float* scan_coords_m,
                   const float* tx_wave_arrivals_s, void* out, uint32_t n_tx, uint32_t n_rx, uint32_t n_samples,
                   uint64_t n_scan, uint32_t n_frames, float f_number, float rx_start_s, float sampling_freq_hz,
                   float sound_speed_m_s, float modulation_freq_hz, float tukey_alpha, int32_t interp_type,
                   float channel_scale, cudaStream_t stream, const mach_b200_options& opt) {
+    if (opt.flags & MACH_B200_FLAG_POWER_DOPPLER) {
+        return power_impl(storage, channel_data, rx_coords_m, scan_coords_m, tx_wave_arrivals_s, out, n_tx, n_rx,
+                          n_samples, n_scan, n_frames, f_number, rx_start_s, sampling_freq_hz, sound_speed_m_s,
+                          modulation_freq_hz, tukey_alpha, interp_type, channel_scale, stream, opt);
+    }
     g_error.clear();
     const uint32_t flags = opt.flags;
     int rc0 = check_args(storage, interp_type, tukey_alpha, n_tx, n_rx, n_samples, n_scan, n_frames);
@@ -734,6 +745,103 @@ mach_b200_options default_options(uint32_t flags) {
 }
 
 
+// ---------------------------------------------------------------- power-Doppler epilogue
+//
+// out (float32 [n_scan]) (+)= sum over frames of |beamformed value|^2.  All-device jobs that
+// the ensemble kernel takes in one launch get the epilogue fused into the kernel (each frame
+// block adds its part atomically); every other job is beamformed into a temporary
+// [n_scan][n_frames] image that one reduction kernel turns into the power image.
+
+int power_impl(int32_t storage, const void* channel_data, const float* rx_coords_m, const float* scan_coords_m,
+               const float* tx_wave_arrivals_s, void* out, uint32_t n_tx, uint32_t n_rx, uint32_t n_samples,
+               uint64_t n_scan, uint32_t n_frames, float f_number, float rx_start_s, float sampling_freq_hz,
+               float sound_speed_m_s, float modulation_freq_hz, float tukey_alpha, int32_t interp_type,
+               float channel_scale, cudaStream_t stream, const mach_b200_options& opt) {
+    g_error.clear();
+    const uint32_t flags = opt.flags;
+    int rc = check_args(storage, interp_type, tukey_alpha, n_tx, n_rx, n_samples, n_scan, n_frames);
+    if (rc) return rc;
+    if (n_scan == 0) return MACH_B200_OK;
+    if (!out || !scan_coords_m) return fail(MACH_B200_ERR_VALUE, "out and scan_coords_m must not be NULL");
+    const bool need_channel = n_tx > 0 && n_rx > 0 && n_samples > 0 && n_frames > 0;
+    if (need_channel && (!channel_data || !rx_coords_m || !tx_wave_arrivals_s)) {
+        return fail(MACH_B200_ERR_VALUE, "channel_data, rx_coords_m and tx_wave_arrivals_s must not be NULL");
+    }
+    int device = 0;
+    MACH_B200_CUDA_TRY(cudaGetDevice(&device));
+    DeviceState* dev = nullptr;
+    if ((rc = device_state(device, &dev))) return rc;
+    Residency r_out;
+    if ((rc = residency(out, device, &r_out, "out"))) return rc;
+    bool all_device = r_out == kOnDevice;
+    if (need_channel) {
+        const void* ptrs[4] = {channel_data, rx_coords_m, scan_coords_m, tx_wave_arrivals_s};
+        const char* names[4] = {"channel_data", "rx_coords_m", "scan_coords_m", "tx_wave_arrivals_s"};
+        for (int i = 0; i < 4; ++i) {
+            Residency r;
+            if ((rc = residency(ptrs[i], device, &r, names[i]))) return rc;
+            all_device = all_device && r == kOnDevice;
+        }
+    }
+    const bool overwrite = (flags & MACH_B200_FLAG_OVERWRITE) != 0u || r_out != kOnDevice;
+    const bool cplx = (storage & 1) != 0;
+    const size_t power_bytes = static_cast<size_t>(n_scan) * sizeof(float);
+
+    // ---- fused: the ensemble kernel adds |x|^2 of each frame block into out
+    if (all_device && need_channel) {
+        Plan plan = plan_launch(storage, n_scan, n_frames, n_tx, channel_data, true, opt, interp_type);
+        const int64_t per_tx = static_cast<int64_t>(n_rx) * n_samples * n_frames;
+        if (plan.ensemble && per_tx * n_tx < (int64_t{1} << 31)) {
+            plan.st.status = dev->status;
+            DasArgs a = make_args(rx_coords_m, scan_coords_m, n_scan, n_rx, n_samples, n_frames, f_number, rx_start_s,
+                                  sampling_freq_hz, sound_speed_m_s, modulation_freq_hz, tukey_alpha, channel_scale,
+                                  cplx, flags);
+            a.frame_passes = plan.lp.passes;
+            a.tx_chunk = plan.lp.tx_chunk;
+            a.channel = channel_data;
+            a.arrivals = tx_wave_arrivals_s;
+            a.out = out;
+            a.n_tx = static_cast<int32_t>(n_tx);
+            a.accumulate = 1;
+            a.power = 1;
+            if (overwrite) MACH_B200_CUDA_TRY(cudaMemsetAsync(out, 0, power_bytes, stream));
+            if ((rc = dispatch_split(storage, a, interp_type, plan, stream))) return rc;
+            if (!(flags & MACH_B200_FLAG_ASYNC)) {
+                MACH_B200_CUDA_TRY(cudaStreamSynchronize(stream));
+                return check_status(dev, stream);
+            }
+            return MACH_B200_OK;
+        }
+    }
+
+    // ---- general: full image into a temporary buffer, then the reduction kernel
+    const size_t image_bytes = static_cast<size_t>(n_scan) * n_frames * (cplx ? 8 : 4);
+    DeviceBuffer image, power;
+    MACH_B200_CUDA_TRY(image.alloc(image_bytes, stream));
+    mach_b200_options o = opt;
+    o.flags = (flags & ~(MACH_B200_FLAG_POWER_DOPPLER | MACH_B200_FLAG_ASYNC)) | MACH_B200_FLAG_OVERWRITE;
+    if (all_device && (flags & MACH_B200_FLAG_ASYNC)) o.flags |= MACH_B200_FLAG_ASYNC;
+    if ((rc = compound_impl(storage, channel_data, rx_coords_m, scan_coords_m, tx_wave_arrivals_s, image.ptr, n_tx,
+                            n_rx, n_samples, n_scan, n_frames, f_number, rx_start_s, sampling_freq_hz,
+                            sound_speed_m_s, modulation_freq_hz, tukey_alpha, interp_type, channel_scale, stream,
+                            o))) {
+        return rc;
+    }
+    float* dst = static_cast<float*>(out);
+    if (r_out != kOnDevice) {
+        MACH_B200_CUDA_TRY(power.alloc(power_bytes, stream));
+        dst = static_cast<float*>(power.ptr);
+    }
+    MACH_B200_CUDA_TRY(launch_power_epilogue(image.ptr, dst, static_cast<int64_t>(n_scan), static_cast<int>(n_frames),
+                                             cplx, !overwrite, stream));
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    if (r_out != kOnDevice) {
+        MACH_B200_CUDA_TRY(cudaMemcpyAsync(out, dst, power_bytes, cudaMemcpyDeviceToHost, stream));
+    }
+    if (!all_device || !(flags & MACH_B200_FLAG_ASYNC)) MACH_B200_CUDA_TRY(cudaStreamSynchronize(stream));
+    return MACH_B200_OK;
+}
+
 // ---------------------------------------------------------------- allocation-free ensemble call
 //
 // mach_b200_beamform_ensemble_noalloc runs the ensemble kernel without allocating anything.
@@ -773,6 +881,9 @@ int noalloc_impl(int32_t storage, const void* channel_data, const float* rx_coor
     const uint32_t flags = opt.flags;
     int rc = check_args(storage, interp_type, tukey_alpha, n_tx, n_rx, n_samples, n_scan, n_frames);
     if (rc) return rc;
+    if (flags & MACH_B200_FLAG_POWER_DOPPLER) {
+        return fail(MACH_B200_ERR_VALUE, "the allocation-free call writes the beamformed frames, not a power image");
+    }
     if (n_scan == 0 || n_frames == 0) return MACH_B200_OK;
     if (!out || !scan_coords_m) return fail(MACH_B200_ERR_VALUE, "out and scan_coords_m must not be NULL");
     const bool need_channel = n_tx > 0 && n_rx > 0 && n_samples > 0;

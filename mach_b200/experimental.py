@@ -79,6 +79,19 @@ def beamform(
         ``out[n_points, n_frames]``: complex64 for complex storage, float32 otherwise.
         A GPU ``out`` is accumulated into; a CPU ``out`` is overwritten (as in mach).
     """
+    return _compound(channel_data, rx_coords_m, scan_coords_m, tx_wave_arrivals_s, out, rx_start_s=rx_start_s,
+                     sampling_freq_hz=sampling_freq_hz, f_number=f_number, sound_speed_m_s=sound_speed_m_s,
+                     modulation_freq_hz=modulation_freq_hz, tukey_alpha=tukey_alpha, interp_type=interp_type,
+                     channel_scale=channel_scale, sync=sync, grid_shape=grid_shape, kernel=kernel,
+                     window_rows=window_rows, lanes_per_voxel=lanes_per_voxel, tx_chunk=tx_chunk, delay=delay,
+                     power=False)
+
+
+def _compound(channel_data, rx_coords_m, scan_coords_m, tx_wave_arrivals_s, out, *, rx_start_s, sampling_freq_hz,
+              f_number, sound_speed_m_s, modulation_freq_hz, tukey_alpha, interp_type, channel_scale, sync, grid_shape,
+              kernel, window_rows, lanes_per_voxel, tx_chunk, delay, power):
+    """Shared body of :func:`beamform` and :func:`mach_b200.doppler.power_doppler` (``power``:
+    ``out`` is the float32 ``[n_points]`` power image instead of the frames)."""
     xp = array_namespace(channel_data)
     complex_pairs = len(channel_data.shape) == 5
     if complex_pairs and channel_data.shape[-1] != 2:
@@ -110,9 +123,10 @@ def beamform(
 
     n_tx, n_rx, n_samples, n_frames = (int(d) for d in channel_data.shape[:4])
     n_points = int(scan_coords_m.shape[0])
-    output_dtype = xp.complex64 if is_complex else xp.float32
+    output_dtype = xp.complex64 if is_complex and not power else xp.float32
+    out_shape = (n_points,) if power else (n_points, n_frames)
     if out is None:
-        out = xp.zeros((n_points, n_frames), dtype=output_dtype, like=channel_data)
+        out = xp.zeros(out_shape, dtype=output_dtype, like=channel_data)
     elif out.dtype != output_dtype:
         raise ValueError(f"Output array dtype {out.dtype} doesn't match expected {output_dtype}")
     if not is_writeable_array(out):
@@ -130,8 +144,8 @@ def beamform(
         raise RuntimeError(f"scan_coords_m.shape {list(scan.shape)} must be [n_points, 3]")
     if tuple(arr.shape) != (n_tx, n_points):
         raise RuntimeError(f"tx_wave_arrivals_s.shape {list(arr.shape)} must be [{n_tx}, {n_points}]")
-    if tuple(o.shape) != (n_points, n_frames):
-        raise RuntimeError(f"out.shape {list(o.shape)} must be [{n_points}, {n_frames}]")
+    if tuple(o.shape) != out_shape:
+        raise RuntimeError(f"out.shape {list(o.shape)} must be {list(out_shape)}")
     cpu = sum(v.device_type == _dlpack.CPU for v in (ch, rx, scan, arr))
     if cpu:
         warnings.warn(
@@ -148,6 +162,8 @@ def beamform(
         raise ValueError(f"delay must be 'auto', 'reference' or 'split', got {delay!r}")
     if delay == "split":
         flags |= _cuda_impl.FLAG_SPLIT_DELAY
+    if power:
+        flags |= _cuda_impl.FLAG_POWER_DOPPLER
     if grid_shape is None:
         grid_shape = _grid.detect(scan_coords_m)
     options = _cuda_impl.make_options(
