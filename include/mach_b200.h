@@ -179,6 +179,20 @@ MACH_B200_API int mach_b200_beamform_ensemble_noalloc(int32_t storage, const voi
                                 int32_t interp_type, float channel_scale, void* cuda_stream,
                                 const mach_b200_options* options);
 
+/*
+ * Channel-data ingest: acquisition order [n_samples][n_elements][n_waves][n_frames] (UFF and
+ * PyMUST order) to the beamformer's [n_waves][n_elements][n_samples][n_frames], converted from
+ * storage `src_storage` to `dst_storage` in the same pass (value x `scale`, rounded to the
+ * destination type; int16 destinations saturate).  Both storages must be real or both
+ * complex (complex: interleaved (I, Q)).  Replaces the einops rearrange and dtype cast of
+ * src/mach/io/uff.py:70-105 and examples/doppler.py:193-195.  `dst` must be device memory;
+ * a host `src` is copied to the device first.  Synchronous unless MACH_B200_FLAG_ASYNC is set
+ * and both buffers are device memory.
+ */
+MACH_B200_API int mach_b200_ingest(int32_t src_storage, const void* src, int32_t dst_storage, void* dst,
+                                   uint32_t n_samples, uint32_t n_elements, uint32_t n_waves,
+                                   uint32_t n_frames, float scale, void* cuda_stream, uint32_t flags);
+
 /* One job of a batch: every pointer must be device memory of the current device. */
 typedef struct mach_b200_job {
     int32_t storage;             /* MACH_B200_STORAGE_* */

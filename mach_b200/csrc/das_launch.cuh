@@ -168,6 +168,11 @@ cudaError_t launch_staged_persistent(int interp, int lanes, const PersistentLaun
 #undef MACH_B200_PST
 }
 
+// Channel-data ingest (das_ingest.cu): (n_s, n_e, n_w, n_frames) -> (n_w, n_e, n_s, n_frames),
+// converted from storage `src_code` to `dst_code` (both real or both complex), times `scale`.
+cudaError_t launch_ingest(int src_code, const void* src, int dst_code, void* dst, int n_s, int n_e, int n_w,
+                          int n_frames, float scale, cudaStream_t st);
+
 // Power-Doppler epilogue (das_power.cu): out[v] (+)= sum over frames of |in[v][f]|^2.
 cudaError_t launch_power_epilogue(const void* in, float* out, int64_t n_vox, int n_frames, bool cplx, bool accumulate,
                                   cudaStream_t stream);

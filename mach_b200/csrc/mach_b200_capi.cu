@@ -842,6 +842,47 @@ int power_impl(int32_t storage, const void* channel_data, const float* rx_coords
     return MACH_B200_OK;
 }
 
+// ---------------------------------------------------------------- channel-data ingest
+
+int ingest_impl(int32_t src_storage, const void* src, int32_t dst_storage, void* dst, uint32_t n_samples,
+                uint32_t n_elements, uint32_t n_waves, uint32_t n_frames, float scale, cudaStream_t stream,
+                uint32_t flags) {
+    g_error.clear();
+    if (src_storage < kF32 || src_storage > kCI16 || dst_storage < kF32 || dst_storage > kCI16) {
+        return fail(MACH_B200_ERR_VALUE, "unknown storage code (%d -> %d)", src_storage, dst_storage);
+    }
+    if ((src_storage & 1) != (dst_storage & 1)) {
+        return fail(MACH_B200_ERR_VALUE, "source and destination must both be real or both be complex");
+    }
+    const uint64_t count = static_cast<uint64_t>(n_samples) * n_elements * n_waves * n_frames;
+    if (count == 0) return MACH_B200_OK;
+    if (!src || !dst) return fail(MACH_B200_ERR_VALUE, "src and dst must not be NULL");
+    if (n_samples > 0x7fffffffu || n_elements > 65535u || n_waves > 0x7fffffffu || n_frames > 0x7fffffffu) {
+        return fail(MACH_B200_ERR_VALUE, "dimensions out of range (at most 65535 elements)");
+    }
+    int device = 0;
+    MACH_B200_CUDA_TRY(cudaGetDevice(&device));
+    Residency r_src, r_dst;
+    int rc;
+    if ((rc = residency(src, device, &r_src, "src"))) return rc;
+    if ((rc = residency(dst, device, &r_dst, "dst"))) return rc;
+    if (r_dst != kOnDevice) return fail(MACH_B200_ERR_VALUE, "dst must be device memory");
+    DeviceBuffer staged;
+    const void* dsrc = src;
+    if (r_src != kOnDevice) {
+        const size_t bytes = count * storage_bytes(src_storage);
+        MACH_B200_CUDA_TRY(staged.alloc(bytes, stream));
+        MACH_B200_CUDA_TRY(cudaMemcpyAsync(staged.ptr, src, bytes, cudaMemcpyHostToDevice, stream));
+        dsrc = staged.ptr;
+    }
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    MACH_B200_CUDA_TRY(launch_ingest(src_storage, dsrc, dst_storage, dst, static_cast<int>(n_samples),
+                                     static_cast<int>(n_elements), static_cast<int>(n_waves),
+                                     static_cast<int>(n_frames), scale, stream));
+    if (r_src != kOnDevice || !(flags & MACH_B200_FLAG_ASYNC)) MACH_B200_CUDA_TRY(cudaStreamSynchronize(stream));
+    return MACH_B200_OK;
+}
+
 // ---------------------------------------------------------------- allocation-free ensemble call
 //
 // mach_b200_beamform_ensemble_noalloc runs the ensemble kernel without allocating anything.
@@ -1284,6 +1325,13 @@ int mach_b200_beamform_ensemble_noalloc(int32_t storage, const void* channel_dat
                         n_samples, n_scan, n_frames, f_number, rx_start_s, sampling_freq_hz, sound_speed_m_s,
                         modulation_freq_hz, tukey_alpha, interp_type, channel_scale,
                         static_cast<cudaStream_t>(cuda_stream), o);
+}
+
+int mach_b200_ingest(int32_t src_storage, const void* src, int32_t dst_storage, void* dst, uint32_t n_samples,
+                     uint32_t n_elements, uint32_t n_waves, uint32_t n_frames, float scale, void* cuda_stream,
+                     uint32_t flags) {
+    return ingest_impl(src_storage, src, dst_storage, dst, n_samples, n_elements, n_waves, n_frames, scale,
+                       static_cast<cudaStream_t>(cuda_stream), flags);
 }
 
 int mach_b200_batch_create(uint32_t max_jobs, mach_b200_batch** batch) { return batch_create(max_jobs, batch); }
