@@ -125,7 +125,10 @@ __device__ __forceinline__ void tmem_st8(uint32_t col, const float2 (&v)[4]) {
                  : "memory");
 }
 // Four loads of (row, row + 1) at columns c0..c3 and the wait for them, in one statement:
-// the outputs are only defined once tcgen05.wait::ld has retired the loads.
+// the outputs are only defined once tcgen05.wait::ld has retired the loads.  No memory
+// clobber: tensor memory is not addressable memory, and the statement stays ordered after
+// the tcgen05.st and fence statements of the copy (all volatile), so shared-memory loads of
+// the next voxels may be scheduled around it.
 __device__ __forceinline__ void tmem_ld4x4(const uint32_t (&c)[4], uint32_t (&r)[4][4]) {
     asm volatile(
         "tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0, %1, %2, %3}, [%16];\n\t"
@@ -136,8 +139,7 @@ __device__ __forceinline__ void tmem_ld4x4(const uint32_t (&c)[4], uint32_t (&r)
         : "=r"(r[0][0]), "=r"(r[0][1]), "=r"(r[0][2]), "=r"(r[0][3]), "=r"(r[1][0]), "=r"(r[1][1]), "=r"(r[1][2]),
           "=r"(r[1][3]), "=r"(r[2][0]), "=r"(r[2][1]), "=r"(r[2][2]), "=r"(r[2][3]), "=r"(r[3][0]), "=r"(r[3][1]),
           "=r"(r[3][2]), "=r"(r[3][3])
-        : "r"(c[0]), "r"(c[1]), "r"(c[2]), "r"(c[3])
-        : "memory");
+        : "r"(c[0]), "r"(c[1]), "r"(c[2]), "r"(c[3]));
 }
 // Same for one row (nearest taps); the second row of each result repeats the first.
 __device__ __forceinline__ void tmem_ld4x2(const uint32_t (&c)[4], uint32_t (&r)[4][4]) {
@@ -149,8 +151,7 @@ __device__ __forceinline__ void tmem_ld4x2(const uint32_t (&c)[4], uint32_t (&r)
         "tcgen05.wait::ld.sync.aligned;"
         : "=r"(r[0][0]), "=r"(r[0][1]), "=r"(r[1][0]), "=r"(r[1][1]), "=r"(r[2][0]), "=r"(r[2][1]), "=r"(r[3][0]),
           "=r"(r[3][1])
-        : "r"(c[0]), "r"(c[1]), "r"(c[2]), "r"(c[3])
-        : "memory");
+        : "r"(c[0]), "r"(c[1]), "r"(c[2]), "r"(c[3]));
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
         r[i][2] = r[i][0];
