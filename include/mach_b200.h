@@ -77,7 +77,8 @@ extern "C" {
 
 /*
  * Optional launch options.  Zero-initialise, set struct_size = sizeof(mach_b200_options),
- * then set what you need.  Every field only affects speed, never the result.
+ * then set what you need.  The launch fields only affect speed, never the result; tx_model
+ * and tx_params replace the arrivals array by its plane / spherical wave model.
  */
 typedef struct mach_b200_options {
     uint32_t struct_size;   /* sizeof(mach_b200_options) */
@@ -89,8 +90,20 @@ typedef struct mach_b200_options {
     int32_t tx_chunk;        /* lane-voxel kernel: transmits per shared-memory pass, 0 = automatic */
     int32_t window_rows;     /* staged / ensemble kernels: sample rows per window, 0 = automatic */
     int32_t lanes_per_voxel; /* staged kernel: 4, 8, 16 or 32, 0 = automatic */
-    int32_t reserved[4];
+    int32_t tx_model;        /* MACH_B200_TX_ARRAYS: read tx_wave_arrivals_s; MACH_B200_TX_PLANE /
+                                MACH_B200_TX_SPHERICAL: compute every (voxel, transmit) arrival on the
+                                device from tx_params (tx_wave_arrivals_s may then be NULL) */
+    int32_t reserved0;
+    const double* tx_params; /* [n_tx][8]: origin xyz (m), unit direction (plane) or focus xyz (m)
+                                (spherical), time offset (s), unused.  The arrival is the distance of
+                                src/mach/wavefront.py:8-116 divided by the sound speed, plus the
+                                offset, formed in FP64 and rounded to FP32.  Device or host memory. */
 } mach_b200_options;
+
+/* Transmit models (mach_b200_options.tx_model). */
+#define MACH_B200_TX_ARRAYS 0
+#define MACH_B200_TX_PLANE 1
+#define MACH_B200_TX_SPHERICAL 2
 
 /*
  * Single-transmit DAS on float32 RF, synchronous on the legacy default stream.

@@ -54,7 +54,9 @@ class Options(ctypes.Structure):
         ("tx_chunk", ctypes.c_int32),
         ("window_rows", ctypes.c_int32),
         ("lanes_per_voxel", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 4),
+        ("tx_model", ctypes.c_int32),
+        ("reserved0", ctypes.c_int32),
+        ("tx_params", ctypes.c_void_p),
     ]
 
 

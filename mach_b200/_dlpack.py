@@ -17,6 +17,12 @@ import numpy as np
 CPU, CUDA, CUDA_HOST, CUDA_MANAGED = 1, 2, 3, 13
 
 
+class NullView:
+    """Stands for an absent array: a NULL pointer."""
+
+    ptr = 0
+
+
 @dataclass
 class ArrayView:
     ptr: int

@@ -452,7 +452,8 @@ int dispatch_split(int storage, DasArgs a, int interp, const Plan& plan, cudaStr
         DasArgs b = a;
         b.n_tx = static_cast<int32_t>(std::min<int64_t>(max_tx, total - t0));
         b.channel = ch + static_cast<size_t>(t0) * per_tx * esz;
-        b.arrivals = arr + static_cast<int64_t>(t0) * a.n_vox;
+        b.arrivals = arr ? arr + static_cast<int64_t>(t0) * a.n_vox : nullptr;
+        b.tx_params = a.tx_params ? a.tx_params + 8 * static_cast<int64_t>(t0) : nullptr;
         b.accumulate = t0 == 0 ? a.accumulate : 1;
         CUtensorMap map;
         std::memset(&map, 0, sizeof(map));
@@ -574,6 +575,40 @@ int check_args(int32_t storage, int32_t interp_type, float tukey_alpha, uint32_t
     return MACH_B200_OK;
 }
 
+// Transmit model of a call: checks, and the device copy of host parameters.  `arrivals_ok`
+// tells whether tx_wave_arrivals_s is needed (model 0) or ignored.
+struct TxModel {
+    int model = 0;
+    const double* params = nullptr;  // device memory
+    DeviceBuffer staged;
+};
+
+int setup_tx_model(const mach_b200_options& o, uint32_t n_tx, int device, cudaStream_t stream, TxModel& tm) {
+    tm.model = o.tx_model;
+    if (tm.model == MACH_B200_TX_ARRAYS) return MACH_B200_OK;
+    if (tm.model != MACH_B200_TX_PLANE && tm.model != MACH_B200_TX_SPHERICAL) {
+        return fail(MACH_B200_ERR_VALUE, "tx_model must be 0 (arrays), 1 (plane) or 2 (spherical), got %d", tm.model);
+    }
+    if (!o.tx_params) return fail(MACH_B200_ERR_VALUE, "tx_model %d needs tx_params", tm.model);
+    Residency r;
+    int rc;
+    if ((rc = residency(o.tx_params, device, &r, "tx_params"))) return rc;
+    tm.params = o.tx_params;
+    if (r != kOnDevice && n_tx > 0) {
+        const size_t bytes = static_cast<size_t>(n_tx) * 8 * sizeof(double);
+        MACH_B200_CUDA_TRY(tm.staged.alloc(bytes, stream));
+        MACH_B200_CUDA_TRY(cudaMemcpyAsync(tm.staged.ptr, o.tx_params, bytes, cudaMemcpyHostToDevice, stream));
+        tm.params = static_cast<const double*>(tm.staged.ptr);
+    }
+    return MACH_B200_OK;
+}
+
+void apply_tx_model(DasArgs& a, const TxModel& tm, float sound_speed_m_s) {
+    a.tx_model = tm.model;
+    a.tx_params = tm.params;
+    a.sound_speed_d = sound_speed_m_s;
+}
+
 int power_impl(int32_t storage, const void* channel_data, const float* rx_coords_m, const float* scan_coords_m,
                const float* tx_wave_arrivals_s, void* out, uint32_t n_tx, uint32_t n_rx, uint32_t n_samples,
                uint64_t n_scan, uint32_t n_frames, float f_number, float rx_start_s, float sampling_freq_hz,
@@ -597,7 +632,8 @@ int compound_impl(int32_t storage, const void* channel_data, const float* rx_coo
     if (n_scan == 0 || n_frames == 0) return MACH_B200_OK;  // empty output: nothing to write
     if (!out || !scan_coords_m) return fail(MACH_B200_ERR_VALUE, "out and scan_coords_m must not be NULL");
     const bool need_channel = n_tx > 0 && n_rx > 0 && n_samples > 0;
-    if (need_channel && (!channel_data || !rx_coords_m || !tx_wave_arrivals_s)) {
+    const bool need_arrivals = opt.tx_model == MACH_B200_TX_ARRAYS;
+    if (need_channel && (!channel_data || !rx_coords_m || (need_arrivals && !tx_wave_arrivals_s))) {
         return fail(MACH_B200_ERR_VALUE, "channel_data, rx_coords_m and tx_wave_arrivals_s must not be NULL");
     }
 
@@ -606,11 +642,13 @@ int compound_impl(int32_t storage, const void* channel_data, const float* rx_coo
     DeviceState* dev = nullptr;
     int rc;
     if ((rc = device_state(device, &dev))) return rc;
+    TxModel tm;
+    if ((rc = setup_tx_model(opt, n_tx, device, stream, tm))) return rc;
     Residency r_ch = kOnDevice, r_rx = kOnDevice, r_scan = kOnDevice, r_arr = kOnDevice, r_out = kOnDevice;
     if (need_channel) {
         if ((rc = residency(channel_data, device, &r_ch, "channel_data"))) return rc;
         if ((rc = residency(rx_coords_m, device, &r_rx, "rx_coords_m"))) return rc;
-        if ((rc = residency(tx_wave_arrivals_s, device, &r_arr, "tx_wave_arrivals_s"))) return rc;
+        if (need_arrivals && (rc = residency(tx_wave_arrivals_s, device, &r_arr, "tx_wave_arrivals_s"))) return rc;
     }
     if ((rc = residency(scan_coords_m, device, &r_scan, "scan_coords_m"))) return rc;
     if ((rc = residency(out, device, &r_out, "out"))) return rc;
@@ -622,6 +660,7 @@ int compound_impl(int32_t storage, const void* channel_data, const float* rx_coo
     DasArgs a = make_args(rx_coords_m, scan_coords_m, n_scan, need_channel ? n_rx : 0, n_samples, n_frames, f_number,
                           rx_start_s, sampling_freq_hz, sound_speed_m_s, modulation_freq_hz, tukey_alpha,
                           channel_scale, cplx, flags);
+    apply_tx_model(a, tm, sound_speed_m_s);
     const bool overwrite = (flags & MACH_B200_FLAG_OVERWRITE) != 0u || r_out != kOnDevice;
     Plan plan = plan_launch(storage, n_scan, n_frames, n_tx, channel_data, r_ch == kOnDevice, opt, interp_type);
     plan.st.status = dev->status;
@@ -717,8 +756,9 @@ int compound_impl(int32_t storage, const void* channel_data, const float* rx_coo
                                                    cudaMemcpyHostToDevice, copy.s));
                 a.arrivals = static_cast<const float*>(d_arr[b].ptr);
             } else {
-                a.arrivals = reinterpret_cast<const float*>(h_arr + arr_bytes * t0);
+                a.arrivals = h_arr ? reinterpret_cast<const float*>(h_arr + arr_bytes * t0) : nullptr;
             }
+            a.tx_params = tm.params ? tm.params + 8 * static_cast<size_t>(t0) : nullptr;
             MACH_B200_CUDA_TRY(cudaEventRecord(copied.ev[b], copy.s));
             MACH_B200_CUDA_TRY(cudaStreamWaitEvent(stream, copied.ev[b], 0));
             a.n_tx = static_cast<int32_t>(nt);
@@ -764,7 +804,8 @@ int power_impl(int32_t storage, const void* channel_data, const float* rx_coords
     if (n_scan == 0) return MACH_B200_OK;
     if (!out || !scan_coords_m) return fail(MACH_B200_ERR_VALUE, "out and scan_coords_m must not be NULL");
     const bool need_channel = n_tx > 0 && n_rx > 0 && n_samples > 0 && n_frames > 0;
-    if (need_channel && (!channel_data || !rx_coords_m || !tx_wave_arrivals_s)) {
+    const bool need_arrivals = opt.tx_model == MACH_B200_TX_ARRAYS;
+    if (need_channel && (!channel_data || !rx_coords_m || (need_arrivals && !tx_wave_arrivals_s))) {
         return fail(MACH_B200_ERR_VALUE, "channel_data, rx_coords_m and tx_wave_arrivals_s must not be NULL");
     }
     int device = 0;
@@ -777,7 +818,7 @@ int power_impl(int32_t storage, const void* channel_data, const float* rx_coords
     if (need_channel) {
         const void* ptrs[4] = {channel_data, rx_coords_m, scan_coords_m, tx_wave_arrivals_s};
         const char* names[4] = {"channel_data", "rx_coords_m", "scan_coords_m", "tx_wave_arrivals_s"};
-        for (int i = 0; i < 4; ++i) {
+        for (int i = 0; i < (need_arrivals ? 4 : 3); ++i) {
             Residency r;
             if ((rc = residency(ptrs[i], device, &r, names[i]))) return rc;
             all_device = all_device && r == kOnDevice;
@@ -796,6 +837,9 @@ int power_impl(int32_t storage, const void* channel_data, const float* rx_coords
             DasArgs a = make_args(rx_coords_m, scan_coords_m, n_scan, n_rx, n_samples, n_frames, f_number, rx_start_s,
                                   sampling_freq_hz, sound_speed_m_s, modulation_freq_hz, tukey_alpha, channel_scale,
                                   cplx, flags);
+            TxModel tm;
+            if ((rc = setup_tx_model(opt, n_tx, device, stream, tm))) return rc;
+            apply_tx_model(a, tm, sound_speed_m_s);
             a.frame_passes = plan.lp.passes;
             a.tx_chunk = plan.lp.tx_chunk;
             a.channel = channel_data;
@@ -928,19 +972,27 @@ int noalloc_impl(int32_t storage, const void* channel_data, const float* rx_coor
     if (n_scan == 0 || n_frames == 0) return MACH_B200_OK;
     if (!out || !scan_coords_m) return fail(MACH_B200_ERR_VALUE, "out and scan_coords_m must not be NULL");
     const bool need_channel = n_tx > 0 && n_rx > 0 && n_samples > 0;
-    if (need_channel && (!channel_data || !rx_coords_m || !tx_wave_arrivals_s)) {
+    const bool need_arrivals = opt.tx_model == MACH_B200_TX_ARRAYS;
+    if (need_channel && (!channel_data || !rx_coords_m || (need_arrivals && !tx_wave_arrivals_s))) {
         return fail(MACH_B200_ERR_VALUE, "channel_data, rx_coords_m and tx_wave_arrivals_s must not be NULL");
     }
     int device = 0;
     MACH_B200_CUDA_TRY(cudaGetDevice(&device));
     DeviceState* dev = nullptr;
     if ((rc = device_state(device, &dev))) return rc;
+    TxModel tm;
+    if (!need_arrivals) {
+        Residency rp = kOnDevice;
+        if (opt.tx_params && (rc = residency(opt.tx_params, device, &rp, "tx_params"))) return rc;
+        if (rp != kOnDevice) return fail(MACH_B200_ERR_VALUE, "tx_params must be device memory for this call");
+        if ((rc = setup_tx_model(opt, n_tx, device, stream, tm))) return rc;  // device params: nothing to copy
+    }
     int* counters = nullptr;
     if ((rc = noalloc_counters(device, &counters))) return rc;
     const void* ptrs[5] = {channel_data, rx_coords_m, scan_coords_m, tx_wave_arrivals_s, out};
     const char* names[5] = {"channel_data", "rx_coords_m", "scan_coords_m", "tx_wave_arrivals_s", "out"};
     for (int i = 0; i < 5; ++i) {
-        if (!ptrs[i]) continue;  // only optional inputs can be NULL here (checked above)
+        if (!ptrs[i] || (i == 3 && !need_arrivals)) continue;  // only optional inputs can be NULL here
         Residency r;
         if ((rc = residency(ptrs[i], device, &r, names[i]))) return rc;
         if (r != kOnDevice) {
@@ -960,10 +1012,11 @@ int noalloc_impl(int32_t storage, const void* channel_data, const float* rx_coor
     DasArgs a = make_args(rx_coords_m, scan_coords_m, n_scan, need_channel ? n_rx : 0, n_samples, n_frames, f_number,
                           rx_start_s, sampling_freq_hz, sound_speed_m_s, modulation_freq_hz, tukey_alpha,
                           channel_scale, cplx, flags);
+    apply_tx_model(a, tm, sound_speed_m_s);
     a.frame_passes = plan.lp.passes;
     a.tx_chunk = plan.lp.tx_chunk;
     a.channel = channel_data;
-    a.arrivals = tx_wave_arrivals_s;
+    a.arrivals = need_arrivals ? tx_wave_arrivals_s : nullptr;
     a.out = out;
     a.n_tx = static_cast<int32_t>(need_channel ? n_tx : 0);
     a.accumulate = (flags & MACH_B200_FLAG_OVERWRITE) ? 0 : 1;
@@ -988,7 +1041,8 @@ int noalloc_impl(int32_t storage, const void* channel_data, const float* rx_coor
         DasArgs b = a;
         b.n_tx = static_cast<int32_t>(std::min<int64_t>(max_tx, total - t0));
         b.channel = ch + static_cast<size_t>(t0) * per_tx * esz;
-        b.arrivals = a.arrivals + static_cast<int64_t>(t0) * a.n_vox;
+        b.arrivals = a.arrivals ? a.arrivals + static_cast<int64_t>(t0) * a.n_vox : nullptr;
+        b.tx_params = a.tx_params ? a.tx_params + 8 * static_cast<int64_t>(t0) : nullptr;
         b.accumulate = t0 == 0 ? a.accumulate : 1;
         CUtensorMap map;
         std::memset(&map, 0, sizeof(map));
@@ -1294,7 +1348,7 @@ int mach_b200_beamform_ex(int32_t storage, const void* channel_data, const float
                           const mach_b200_options* options) {
     mach_b200_options o = default_options(0u);
     if (options) {
-        if (options->struct_size < offsetof(mach_b200_options, reserved)) {
+        if (options->struct_size < offsetof(mach_b200_options, tx_model)) {
             g_error = "mach_b200_options.struct_size is too small";
             return MACH_B200_ERR_VALUE;
         }
@@ -1315,7 +1369,7 @@ int mach_b200_beamform_ensemble_noalloc(int32_t storage, const void* channel_dat
                                         const mach_b200_options* options) {
     mach_b200_options o = default_options(0u);
     if (options) {
-        if (options->struct_size < offsetof(mach_b200_options, reserved)) {
+        if (options->struct_size < offsetof(mach_b200_options, tx_model)) {
             g_error = "mach_b200_options.struct_size is too small";
             return MACH_B200_ERR_VALUE;
         }

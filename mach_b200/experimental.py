@@ -114,12 +114,28 @@ def _compound(channel_data, rx_coords_m, scan_coords_m, tx_wave_arrivals_s, out,
     if modulation_freq_hz is None:
         modulation_freq_hz = 0.0
 
+    from mach_b200.wavefront import TransmitWaves
+
     xpc = array_namespace(rx_coords_m)
     xps = array_namespace(scan_coords_m)
-    xpa = array_namespace(tx_wave_arrivals_s)
     rx_coords_m = ensure_contiguous(xpc.astype(rx_coords_m, xpc.float32, copy=False))
     scan_coords_m = ensure_contiguous(xps.astype(scan_coords_m, xps.float32, copy=False))
-    tx_wave_arrivals_s = ensure_contiguous(xpa.astype(tx_wave_arrivals_s, xpa.float32, copy=False))
+    waves = tx_wave_arrivals_s if isinstance(tx_wave_arrivals_s, TransmitWaves) else None
+    if waves is None:
+        xpa = array_namespace(tx_wave_arrivals_s)
+        tx_wave_arrivals_s = ensure_contiguous(xpa.astype(tx_wave_arrivals_s, xpa.float32, copy=False))
+    else:
+        if waves.n_transmits != int(channel_data.shape[0]):
+            raise RuntimeError(f"{waves.n_transmits} transmit waves for {int(channel_data.shape[0])} transmits")
+        # FP64 wave table next to the channel data (device tensor for torch CUDA input)
+        if _dlpack.is_torch(channel_data) and channel_data.device.type == "cuda":
+            import torch
+
+            tx_wave_arrivals_s = torch.as_tensor(waves.table, device=channel_data.device)
+        else:
+            import numpy as np
+
+            tx_wave_arrivals_s = np.ascontiguousarray(waves.table)
 
     n_tx, n_rx, n_samples, n_frames = (int(d) for d in channel_data.shape[:4])
     n_points = int(scan_coords_m.shape[0])
@@ -136,13 +152,13 @@ def _compound(channel_data, rx_coords_m, scan_coords_m, tx_wave_arrivals_s, out,
 
     rx = _dlpack.view(rx_coords_m)
     scan = _dlpack.view(scan_coords_m)
-    arr = _dlpack.view(tx_wave_arrivals_s)
+    arr = _dlpack.view(tx_wave_arrivals_s)  # the wave table when `waves` is given
     o = _dlpack.view(out)
     if tuple(rx.shape) != (n_rx, 3):
         raise RuntimeError(f"rx_coords_m.shape {list(rx.shape)} must be [{n_rx}, 3]")
     if tuple(scan.shape) != (n_points, 3):
         raise RuntimeError(f"scan_coords_m.shape {list(scan.shape)} must be [n_points, 3]")
-    if tuple(arr.shape) != (n_tx, n_points):
+    if waves is None and tuple(arr.shape) != (n_tx, n_points):
         raise RuntimeError(f"tx_wave_arrivals_s.shape {list(arr.shape)} must be [{n_tx}, {n_points}]")
     if tuple(o.shape) != out_shape:
         raise RuntimeError(f"out.shape {list(o.shape)} must be {list(out_shape)}")
@@ -169,6 +185,10 @@ def _compound(channel_data, rx_coords_m, scan_coords_m, tx_wave_arrivals_s, out,
     options = _cuda_impl.make_options(
         flags, grid_shape=grid_shape or None, kernel=kernel, tx_chunk=tx_chunk, window_rows=window_rows,
         lanes_per_voxel=lanes_per_voxel)
+    if waves is not None:
+        options.tx_model = waves.model
+        options.tx_params = arr.ptr
+        arr = _dlpack.NullView()
     _cuda_impl.beamform_compound(
         ch, storage, rx, scan, arr, o, n_tx=n_tx, n_rx=n_rx, n_samples=n_samples, n_vox=n_points,
         n_frames=n_frames, f_number=f_number, rx_start_s=rx_start_s, sampling_freq_hz=sampling_freq_hz,

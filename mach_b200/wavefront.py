@@ -40,3 +40,75 @@ def spherical(origin_m: Any, points_m: Any, focus_m: Any) -> Any:
     origin_sign = xp.sign(focus_m[2] - origin_m[2])
     point_sign = xp.sign(focus_m[2] - points_m[..., 2])
     return origin_focus * origin_sign - focus_point * point_sign
+
+
+class TransmitWaves:
+    """Transmit wavefronts that the beamformer evaluates on the GPU.
+
+    Pass an instance as ``tx_wave_arrivals_s`` of :func:`mach_b200.experimental.beamform`
+    (or :func:`mach_b200.doppler.power_doppler`) instead of the ``[n_transmits, n_points]``
+    arrivals array: each (point, transmit) arrival is then computed inside the kernel from
+    the wave's origin and direction or focus, in FP64 and rounded to FP32, the same as
+    ``plane(...) / sound_speed`` or ``spherical(...) / sound_speed`` evaluated on the host.
+    The array (4 bytes per point and transmit, 79 MB for 75 transmits on 512x512) is never
+    formed, copied or read.
+    """
+
+    model = 0
+
+    def __init__(self, origin_m: Any, vectors: Any, time_offset_s: Any = 0.0):
+        import numpy as np
+
+        origin = np.asarray(origin_m, dtype=np.float64)
+        vec = np.atleast_2d(np.asarray(vectors, dtype=np.float64))
+        n = vec.shape[0]
+        origin = np.broadcast_to(origin, (n, 3))
+        offset = np.broadcast_to(np.asarray(time_offset_s, dtype=np.float64), (n,))
+        self.table = np.zeros((n, 8), dtype=np.float64)
+        self.table[:, 0:3] = origin
+        self.table[:, 3:6] = vec
+        self.table[:, 6] = offset
+
+    @property
+    def n_transmits(self) -> int:
+        return int(self.table.shape[0])
+
+    def __len__(self) -> int:
+        return self.n_transmits
+
+    def arrivals(self, points_m: Any, sound_speed_m_s: float) -> Any:
+        """The ``[n_transmits, n_points]`` float64 arrivals the GPU computes, on the host."""
+        import numpy as np
+
+        pts = np.asarray(points_m, dtype=np.float64)
+        rows = [self._distance(row[0:3], pts, row[3:6]) / sound_speed_m_s + row[6] for row in self.table]
+        return np.stack(rows)
+
+
+class PlaneWaves(TransmitWaves):
+    """Plane waves: ``origin_m`` ``[3]`` or ``[n, 3]``, unit ``directions`` ``[n, 3]``."""
+
+    model = 1
+
+    def __init__(self, origin_m: Any, directions: Any, time_offset_s: Any = 0.0):
+        import numpy as np
+
+        d = np.atleast_2d(np.asarray(directions, dtype=np.float64))
+        if not np.all(np.abs(np.linalg.norm(d, axis=-1) - 1) < 1e-6):
+            raise ValueError("direction must be a unit vector")
+        super().__init__(origin_m, d, time_offset_s)
+
+    @staticmethod
+    def _distance(origin, points, direction):
+        return plane(origin, points, direction)
+
+
+class SphericalWaves(TransmitWaves):
+    """Focused or diverging waves: ``origin_m`` ``[3]`` or ``[n, 3]``, ``foci_m`` ``[n, 3]``."""
+
+    model = 2
+
+    @staticmethod
+    def _distance(origin, points, focus):
+        return spherical(origin, points, focus)
+

@@ -73,3 +73,22 @@ def test_spherical_to_cartesian():
     x, y, z = geometry.spherical_to_cartesian(math.pi / 4, math.pi / 3, 2.0)
     assert (x, y, z) == pytest.approx((2 * math.sin(math.pi / 4) * 0.5, 2 * math.sin(math.pi / 4) * math.sin(math.pi / 3),
                                        2 * math.cos(math.pi / 4)))
+
+
+def test_transmit_wave_tables():
+    dirs = geometry.ultrasound_angles_to_cartesian(np.deg2rad([-10.0, 0.0, 10.0]), np.zeros(3))
+    waves = wavefront.PlaneWaves(np.array([0.0, 0.0, 1e-3]), dirs, time_offset_s=[1e-6, 0.0, 2e-6])
+    assert waves.model == 1 and len(waves) == 3 and waves.table.shape == (3, 8)
+    np.testing.assert_array_equal(waves.table[:, 0:3], [[0.0, 0.0, 1e-3]] * 3)
+    np.testing.assert_array_equal(waves.table[:, 3:6], dirs)
+    np.testing.assert_array_equal(waves.table[:, 6], [1e-6, 0.0, 2e-6])
+    pts = np.random.default_rng(1).normal(scale=1e-2, size=(20, 3))
+    want = np.stack([wavefront.plane([0.0, 0.0, 1e-3], pts, d) / 1540.0 for d in dirs]) + np.array([[1e-6], [0], [2e-6]])
+    np.testing.assert_allclose(waves.arrivals(pts, 1540.0), want, rtol=0, atol=1e-18)
+    with pytest.raises(ValueError):
+        wavefront.PlaneWaves(np.zeros(3), [[0.0, 0.0, 2.0]])
+    foci = np.array([[0.0, 0.0, 2e-2], [1e-3, 0.0, -5e-3]])
+    sw = wavefront.SphericalWaves(np.zeros(3), foci)
+    assert sw.model == 2
+    np.testing.assert_allclose(sw.arrivals(pts, 1500.0),
+                               np.stack([wavefront.spherical(np.zeros(3), pts, f) / 1500.0 for f in foci]))
