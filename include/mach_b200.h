@@ -206,6 +206,27 @@ MACH_B200_API int mach_b200_ingest(int32_t src_storage, const void* src, int32_t
                                    uint32_t n_samples, uint32_t n_elements, uint32_t n_waves,
                                    uint32_t n_frames, float scale, void* cuda_stream, uint32_t flags);
 
+/* Layouts of the real channel data given to mach_b200_hilbert. */
+#define MACH_B200_LAYOUT_CHANNEL 0     /* [n_waves][n_elements][n_samples][n_frames] */
+#define MACH_B200_LAYOUT_ACQUISITION 1 /* [n_samples][n_elements][n_waves][n_frames] (UFF, PyMUST) */
+
+/*
+ * RF -> IQ by the analytic signal: dst = x + i H{x} along the sample axis of real channel data,
+ * the result of scipy.signal.hilbert(x, axis=samples) (src/mach/io/uff.py:88, mach's front end
+ * for modulation frequency 0; beamform the result with modulation_freq_hz = 0).  `src` is real
+ * storage (F32, F16, BF16, I16) in `src_layout`; `dst` is complex storage (C64, CF16, CBF16,
+ * CI16; interleaved (I, Q)) in the channel layout [n_waves][n_elements][n_samples][n_frames],
+ * so MACH_B200_LAYOUT_ACQUISITION also does the rearrange of src/mach/io/uff.py:101-102.  Both
+ * parts are multiplied by `scale` before rounding (int16 saturates).  Transforms are computed
+ * in FP32 with exact twiddles; n_samples is at most (227 KB / 24 bytes) on B200.  `dst` must be
+ * device memory and must not overlap `src`; a host `src` is copied to the device first.
+ * Synchronous unless MACH_B200_FLAG_ASYNC is set and `src` is device memory.
+ */
+MACH_B200_API int mach_b200_hilbert(int32_t src_storage, const void* src, int32_t src_layout,
+                                    int32_t dst_storage, void* dst, uint32_t n_samples,
+                                    uint32_t n_elements, uint32_t n_waves, uint32_t n_frames,
+                                    float scale, void* cuda_stream, uint32_t flags);
+
 /* One job of a batch: every pointer must be device memory of the current device. */
 typedef struct mach_b200_job {
     int32_t storage;             /* MACH_B200_STORAGE_* */

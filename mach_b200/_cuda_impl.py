@@ -85,6 +85,10 @@ _lib.mach_b200_beamform_ex.argtypes = [
 _lib.mach_b200_beamform_ex.restype = ctypes.c_int
 _lib.mach_b200_ingest.argtypes = [_I32, _P, _I32, _P, _U32, _U32, _U32, _U32, _F, _P, _U32]
 _lib.mach_b200_ingest.restype = ctypes.c_int
+_lib.mach_b200_hilbert.argtypes = [_I32, _P, _I32, _I32, _P, _U32, _U32, _U32, _U32, _F, _P, _U32]
+_lib.mach_b200_hilbert.restype = ctypes.c_int
+LAYOUT_CHANNEL = 0
+LAYOUT_ACQUISITION = 1
 _lib.mach_b200_last_error.restype = ctypes.c_char_p
 _lib.mach_b200_nvcc_version.restype = ctypes.c_char_p
 _lib.mach_b200_version.restype = ctypes.c_char_p

@@ -173,6 +173,39 @@ cudaError_t launch_staged_persistent(int interp, int lanes, const PersistentLaun
 cudaError_t launch_ingest(int src_code, const void* src, int dst_code, void* dst, int n_s, int n_e, int n_w,
                           int n_frames, float scale, cudaStream_t st);
 
+// Analytic signal along the sample axis (das_hilbert.cu).  Column c of the real source splits
+// into (c2, c1, c0) with c0 = c % n0, c1 = (c / n0) % n1, c2 = c / (n0 n1); its sample s sits at
+// element sum(c_i * src_stride[i]) + s * src_sample, and its complex result at
+// sum(c_i * dst_stride[i]) + s * dst_sample (in complex elements).
+constexpr int kHilMaxStages = 32;
+struct HilbertArgs {
+    const void* src;
+    void* dst;
+    int n;                    // samples per column: the transform length
+    int n_stages;             // Stockham stages; radix[s] of each
+    int radix[kHilMaxStages];
+    float inv_n;              // 1 / n
+    float scale;              // both parts of the result are multiplied by it before rounding
+    int64_t n_cols;
+    int cols_per_cta;         // even: columns are transformed in pairs
+    int load_cols_fast;       // 1: consecutive threads read consecutive columns of one sample
+    int store_cols_fast;      // 1: consecutive threads write consecutive columns of one sample
+    int64_t n0, n1;
+    int64_t src_stride[3];
+    int64_t src_sample;
+    int64_t dst_stride[3];
+    int64_t dst_sample;
+};
+
+// Radices of the Stockham stages for length n (8, 4, 2 first, then odd primes); -1 if more
+// than max_stages.
+int hilbert_plan(int n, int* radix, int max_stages);
+
+// Real storage src_code (kF32/kF16/kBF16/kI16) to complex dst_code (kC64/kCF16/kCBF16/kCI16);
+// `smem` = 8 n (cols_per_cta + 1) bytes.
+cudaError_t launch_hilbert(int src_code, int dst_code, const HilbertArgs& g, int blocks, size_t smem,
+                           cudaStream_t st);
+
 // Power-Doppler epilogue (das_power.cu): out[v] (+)= sum over frames of |in[v][f]|^2.
 cudaError_t launch_power_epilogue(const void* in, float* out, int64_t n_vox, int n_frames, bool cplx, bool accumulate,
                                   cudaStream_t stream);

@@ -927,6 +927,96 @@ int ingest_impl(int32_t src_storage, const void* src, int32_t dst_storage, void*
     return MACH_B200_OK;
 }
 
+// ---------------------------------------------------------------- analytic signal (RF -> IQ)
+//
+// scipy.signal.hilbert along the sample axis (src/mach/io/uff.py:88), from the channel layout
+// or fused with the acquisition-order rearrange of src/mach/io/uff.py:101-102.
+
+int hilbert_impl(int32_t src_storage, const void* src, int32_t src_layout, int32_t dst_storage, void* dst,
+                 uint32_t n_samples, uint32_t n_elements, uint32_t n_waves, uint32_t n_frames, float scale,
+                 cudaStream_t stream, uint32_t flags) {
+    g_error.clear();
+    if (src_storage < kF32 || src_storage > kCI16 || dst_storage < kF32 || dst_storage > kCI16) {
+        return fail(MACH_B200_ERR_VALUE, "unknown storage code (%d -> %d)", src_storage, dst_storage);
+    }
+    if ((src_storage & 1) || !(dst_storage & 1)) {
+        return fail(MACH_B200_ERR_VALUE, "the analytic signal takes real channel data to a complex storage");
+    }
+    if (src_layout != MACH_B200_LAYOUT_CHANNEL && src_layout != MACH_B200_LAYOUT_ACQUISITION) {
+        return fail(MACH_B200_ERR_VALUE, "src_layout must be 0 (channel) or 1 (acquisition), got %d", src_layout);
+    }
+    const uint64_t count = static_cast<uint64_t>(n_samples) * n_elements * n_waves * n_frames;
+    if (count == 0) return MACH_B200_OK;
+    if (!src || !dst) return fail(MACH_B200_ERR_VALUE, "src and dst must not be NULL");
+    HilbertArgs g{};
+    g.n = static_cast<int>(std::min<uint32_t>(n_samples, 0x7fffffffu));
+    g.n_stages = hilbert_plan(g.n, g.radix, kHilMaxStages);
+    if (g.n_stages < 0) return fail(MACH_B200_ERR_VALUE, "n_samples %u has too many factors", n_samples);
+    int device = 0;
+    MACH_B200_CUDA_TRY(cudaGetDevice(&device));
+    int max_smem = 0, n_sm = 0;
+    MACH_B200_CUDA_TRY(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
+    MACH_B200_CUDA_TRY(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, device));
+    // Shared memory: twiddle table + two buffers of one complex column per column pair.
+    const uint64_t col_bytes = 8ull * g.n;
+    const uint64_t two_per_sm = 113ull << 10;
+    if (col_bytes * 3 > static_cast<uint64_t>(max_smem)) {
+        return fail(MACH_B200_ERR_VALUE, "n_samples %u is too long for the on-device analytic signal (at most %d)",
+                    n_samples, max_smem / 24);
+    }
+    const int64_t n_cols = static_cast<int64_t>(n_elements) * n_waves * n_frames;
+    int cols = 2;
+    while (cols < 16 && col_bytes * (cols + 3) <= two_per_sm && cols < n_cols) cols += 2;
+    g.cols_per_cta = cols;
+    const size_t smem = static_cast<size_t>(col_bytes * (cols + 1));
+    g.n_cols = n_cols;
+    g.inv_n = 1.0f / static_cast<float>(g.n);
+    g.scale = scale;
+    const int64_t N = g.n, F = n_frames, E = n_elements, W = n_waves;
+    g.n0 = F;
+    if (src_layout == MACH_B200_LAYOUT_CHANNEL) {  // c = (w, e, f); [W][E][N][F] on both sides
+        g.n1 = E;
+        g.src_stride[0] = 1;
+        g.src_stride[1] = N * F;
+        g.src_stride[2] = E * N * F;
+        g.src_sample = F;
+    } else {  // c = (e, w, f); source [N][E][W][F]
+        g.n1 = W;
+        g.src_stride[0] = 1;
+        g.src_stride[1] = F;
+        g.src_stride[2] = W * F;
+        g.src_sample = E * W * F;
+    }
+    g.dst_stride[0] = 1;
+    g.dst_stride[1] = src_layout == MACH_B200_LAYOUT_CHANNEL ? N * F : E * N * F;  // e or w
+    g.dst_stride[2] = src_layout == MACH_B200_LAYOUT_CHANNEL ? E * N * F : N * F;  // w or e
+    g.dst_sample = F;
+    g.load_cols_fast = g.src_sample != 1;
+    g.store_cols_fast = g.dst_sample != 1;
+
+    Residency r_src, r_dst;
+    int rc;
+    if ((rc = residency(src, device, &r_src, "src"))) return rc;
+    if ((rc = residency(dst, device, &r_dst, "dst"))) return rc;
+    if (r_dst != kOnDevice) return fail(MACH_B200_ERR_VALUE, "dst must be device memory");
+    DeviceBuffer staged;
+    g.src = src;
+    if (r_src != kOnDevice) {
+        const size_t bytes = count * storage_bytes(src_storage);
+        MACH_B200_CUDA_TRY(staged.alloc(bytes, stream));
+        MACH_B200_CUDA_TRY(cudaMemcpyAsync(staged.ptr, src, bytes, cudaMemcpyHostToDevice, stream));
+        g.src = staged.ptr;
+    }
+    g.dst = dst;
+    const int64_t groups = (n_cols + cols - 1) / cols;
+    const int per_sm = std::max<int>(1, static_cast<int>(std::min<uint64_t>(2, (228ull << 10) / (smem + 1024))));
+    const int blocks = static_cast<int>(std::min<int64_t>(groups, static_cast<int64_t>(n_sm) * per_sm));
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    MACH_B200_CUDA_TRY(launch_hilbert(src_storage, dst_storage, g, blocks, smem, stream));
+    if (r_src != kOnDevice || !(flags & MACH_B200_FLAG_ASYNC)) MACH_B200_CUDA_TRY(cudaStreamSynchronize(stream));
+    return MACH_B200_OK;
+}
+
 // ---------------------------------------------------------------- allocation-free ensemble call
 //
 // mach_b200_beamform_ensemble_noalloc runs the ensemble kernel without allocating anything.
@@ -1386,6 +1476,13 @@ int mach_b200_ingest(int32_t src_storage, const void* src, int32_t dst_storage, 
                      uint32_t flags) {
     return ingest_impl(src_storage, src, dst_storage, dst, n_samples, n_elements, n_waves, n_frames, scale,
                        static_cast<cudaStream_t>(cuda_stream), flags);
+}
+
+int mach_b200_hilbert(int32_t src_storage, const void* src, int32_t src_layout, int32_t dst_storage, void* dst,
+                      uint32_t n_samples, uint32_t n_elements, uint32_t n_waves, uint32_t n_frames, float scale,
+                      void* cuda_stream, uint32_t flags) {
+    return hilbert_impl(src_storage, src, src_layout, dst_storage, dst, n_samples, n_elements, n_waves, n_frames,
+                        scale, static_cast<cudaStream_t>(cuda_stream), flags);
 }
 
 int mach_b200_batch_create(uint32_t max_jobs, mach_b200_batch** batch) { return batch_create(max_jobs, batch); }
