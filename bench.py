@@ -6,7 +6,11 @@ coherent compounding, 128 elements, 512x512 grid, 3328 complex64 IQ samples, qua
 interpolation, f# 1.75) with every input already in HBM.  Prints ONE JSON line on rank 0.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--workload compound|doppler|plain2d|volume3d|volume3d16] [--storage c64|cf16|...]
+                  [--workload compound|doppler|plain2d|volume3d|volume3d16|serving|rf2iq|ingest]
+                  [--storage c64|cf16|...]
+
+rf2iq and ingest time the front end before the beamformer (RF -> IQ by the analytic signal,
+and the acquisition-order rearrange) in channel samples/s.
 
 --impl reference times mach's own CUDA kernel (built from its unmodified source into
 oracle/_ref) on the same inputs, driven as mach drives it: one launch and one
@@ -45,9 +49,16 @@ WORKLOAD_DESC = {
     "plain2d": "single 0 deg plane wave, 128 el, 256x256 grid, 2048 float32 RF samples, linear, Hann f# 1.5",
     "volume3d": "9 diverging waves, 32x32 matrix array, 128^3 grid, 2048 int16 RF samples, 1 frame, linear, f# 1.0",
     "volume3d16": "9 diverging waves, 32x32 matrix array, 128^3 grid, 2048 int16 RF samples, 16 frames, linear, f# 1.0",
+    "rf2iq": "RF -> IQ front end (src/mach/io/uff.py:70-105 at modulation 0): float32 RF in acquisition order "
+             "[3328 samples, 128 elements, 75 waves] -> analytic signal, complex64 in the beamformer's layout",
+    "ingest": "Doppler channel-data ingest (examples/doppler.py:193-195): complex64 IQ in acquisition order "
+              "[1024 samples, 128 elements, 5 waves, 200 frames] -> the beamformer's layout",
     "serving": "Poisson 2000 req/s (seed 4): 50% plain 2-D 256^2, 30% 75-tx compounding 384^2, 15% 32-frame Doppler "
                "256^2, 5% 3-D 1024-ch 96^3; FP16 storage, FP32 accumulation; resident data, continuous batching",
 }
+
+FRONTEND_SHAPES = {"rf2iq": (3328, 128, 75, 1), "ingest": (1024, 128, 5, 200)}  # acquisition order
+FRONTEND_METRIC = "samples/s (channel samples through the front-end step)"
 
 SERVING_RATE_HZ = 2000.0
 SERVING_REQUESTS_PER_STEP = 100  # one step = 100 requests of the stream (50 ms of arrivals)
@@ -599,6 +610,177 @@ def run_serving_reference(args, world, rank, local):
     }
 
 
+# ----------------------------------------------------------------------------- front end (RF -> IQ, ingest)
+
+
+def frontend_input(name: str, device) -> torch.Tensor:
+    """Seeded acquisition-order channel data: Gaussian RF (rf2iq) or IQ (ingest) samples."""
+    g = torch.Generator(device=device).manual_seed(11)
+    shape = FRONTEND_SHAPES[name]
+    if name == "rf2iq":
+        return torch.randn(shape, device=device, generator=g)
+    return torch.complex(torch.randn(shape, device=device, generator=g), torch.randn(shape, device=device, generator=g))
+
+
+def frontend_reference_step(name: str, x: np.ndarray) -> np.ndarray:
+    """What mach runs on the host for this step: scipy.signal.hilbert on axis 0 then the einops
+    rearrange (src/mach/io/uff.py:86-105), or the rearrange with the complex64 cast
+    (examples/doppler.py:193-195)."""
+    import einops
+
+    pattern = "n_samples n_elements n_waves n_frames -> n_waves n_elements n_samples n_frames"
+    if name == "rf2iq":
+        import scipy.signal
+
+        return np.asarray(einops.rearrange(scipy.signal.hilbert(x, axis=0), pattern))
+    return np.ascontiguousarray(einops.rearrange(x, pattern), dtype=np.complex64)
+
+
+def run_frontend(args, world, rank, local):
+    """One step = the whole front-end job of the workload on the GPU (one kernel launch)."""
+    from mach_b200 import _cuda_impl, ingest
+    from oracle import analytic
+
+    dev = torch.device("cuda", local)
+    x = frontend_input(args.workload, dev)
+    n_s, n_e, n_w, n_f = FRONTEND_SHAPES[args.workload]
+    storage = args.storage or "c64"
+
+    def run(src, out=None, sync=False):
+        if args.workload == "rf2iq":
+            return ingest.preprocess_signal(src, 0.0, storage=storage, out=out, sync=sync)
+        return ingest.ingest(src, storage, out=out, sync=sync)
+
+    out = run(x)
+    torch.cuda.synchronize()
+    samples = x.numel()
+    alg = x.numel() * x.element_size() + out.numel() * out.element_size()
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    for _ in range(args.warmup):
+        run(x, out)
+    torch.cuda.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    launches0 = _cuda_impl.launch_count()
+    stream = torch.cuda.current_stream(dev)
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    for i in range(args.steps):
+        starts[i].record(stream)
+        run(x, out)
+        ends[i].record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    launches = _cuda_impl.launch_count() - launches0
+    clock_info = clocks.stop()
+    per_step = [a.elapsed_time(b) for a, b in zip(starts, ends)]
+    total_ms = max_over_ranks(starts[0].elapsed_time(ends[-1]), world)
+    kernel_s = statistics.mean(per_step) / 1e3
+    peak, peak_kind = measured_peak_hbm()
+    achieved = alg / kernel_s / 1e9
+    line = {
+        "metric": FRONTEND_METRIC, "value": world * samples * args.steps / (total_ms / 1e3), "unit": "samples/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32" if args.workload == "rf2iq" else "c64",
+        "data": "synthetic (seeded Gaussian channel samples; no public dataset offline)",
+        "config": {"workload": f"{args.workload}: {WORKLOAD_DESC[args.workload]}", "storage_out": storage,
+                   "shape_in": [n_s, n_e, n_w, n_f], "samples_per_step": samples,
+                   "l2": f"inputs larger than L2 ({alg / 1e6:.0f} MB per step > 126 MB), no flush",
+                   "parallelism": f"replicas x{world} (one job per GPU, no exchange)"},
+        "latency_ms": {"p50": float(np.percentile(per_step, 50)), "p99": float(np.percentile(per_step, 99))},
+        "gpu_launches": int(launches),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": profiled_traffic(f"{args.workload}:{storage}"), "algorithmic_bytes_per_launch": alg,
+                     "kernel_ms": kernel_s * 1e3, "peak_source": peak_kind},
+        "clocks": clock_info,
+    }
+    if not args.no_e2e:  # pinned host input -> GPU -> pinned host output, through the public API
+        x_h = x.cpu().pin_memory()
+        out_h = torch.empty(out.shape, dtype=out.dtype).pin_memory()
+
+        def e2e_step():
+            run(x_h, out)
+            out_h.copy_(out, non_blocking=True)
+            torch.cuda.current_stream(dev).synchronize()
+
+        e2e_step()
+        barrier(world)
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            e2e_step()
+        dt = max_over_ranks(time.perf_counter() - t0, world)
+        line["e2e"] = {"value": world * samples * args.steps / dt, "unit": "samples/s",
+                       "h2d_bytes_per_step": int(x_h.numel() * x_h.element_size()),
+                       "d2h_bytes_per_step": int(out_h.numel() * out_h.element_size()),
+                       "ms_per_step": dt / args.steps * 1e3, "api": "mach_b200.ingest with pinned host tensors"}
+    if rank == 0 and world == 1:
+        # accuracy against the FP64 oracle and the CPU baseline (mach's host step), on a sample of waves
+        x_np = x.cpu().numpy()
+        got = out.cpu().numpy()
+        if got.ndim == 5:
+            got = got[..., 0] + 1j * got[..., 1]
+
+        def host(n_take):
+            t0 = time.perf_counter()
+            r = frontend_reference_step(args.workload, x_np[:, :, :n_take])
+            return r, time.perf_counter() - t0
+
+        n_take = 1
+        ref, dt = host(n_take)
+        while dt < 0.25 * args.cpu_seconds and n_take < n_w:
+            n_take = min(n_w, max(n_take + 1, int(n_take * 0.5 * args.cpu_seconds / max(dt, 1e-3))))
+            ref, dt = host(n_take)
+        reps = 1
+        if dt < 0.25 * args.cpu_seconds:
+            reps = int(min(100, np.ceil(0.5 * args.cpu_seconds / max(dt, 1e-4))))
+            t0 = time.perf_counter()
+            for _ in range(reps):
+                host(n_take)
+            dt = time.perf_counter() - t0
+        if not args.no_cpu_baseline:
+            what = "scipy.signal.hilbert + einops rearrange" if args.workload == "rf2iq" else \
+                "einops rearrange + complex64 cast"
+            line["cpu_baseline"] = {
+                "value": n_s * n_e * n_take * n_f * reps / dt, "unit": "samples/s", "cores": 1, "kind": "reference",
+                "sample": f"{n_take} of {n_w} waves{f', {reps} passes' if reps > 1 else ''}: mach's host step "
+                          f"({what}), {dt:.1f} s"}
+        want = analytic.preprocess_signal(x_np[:, :, :n_take]) if args.workload == "rf2iq" else ref
+        line["accuracy"] = {"rel_l2_vs_fp64_oracle": float(np.linalg.norm(got[:n_take] - want) / np.linalg.norm(want)),
+                            "waves_checked": n_take}
+    return line
+
+
+def run_frontend_reference(args, world, rank, local):
+    """mach's host implementation of the front-end step (scipy / einops / NumPy), whole job per step."""
+    x = frontend_input(args.workload, torch.device("cuda", local)).cpu().numpy()
+    n_s, n_e, n_w, n_f = FRONTEND_SHAPES[args.workload]
+    for _ in range(min(args.warmup, 1)):
+        frontend_reference_step(args.workload, x)
+    lat = []
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        s = time.perf_counter()
+        frontend_reference_step(args.workload, x)
+        lat.append((time.perf_counter() - s) * 1e3)
+    dt = time.perf_counter() - t0
+    value = x.size * args.steps / dt
+    return {"metric": FRONTEND_METRIC, "value": value, "unit": "samples/s", "impl": "reference", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if args.workload == "rf2iq" else "c64",
+            "data": "synthetic (seeded Gaussian channel samples; no public dataset offline)",
+            "config": {"workload": f"{args.workload}: {WORKLOAD_DESC[args.workload]}", "shape_in": [n_s, n_e, n_w, n_f],
+                       "parallelism": "rank 0 only, host cores"},
+            "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
+            "cpu_baseline": {"value": value, "unit": "samples/s", "cores": 1, "kind": "reference",
+                             "sample": "the whole job per step"},
+            "e2e": {"value": value, "unit": "samples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
 # ----------------------------------------------------------------------------- reference arm
 
 
@@ -697,9 +879,11 @@ def main():
         if args.impl == "reference":
             if rank != 0:
                 return
-            line = (run_serving_reference if args.workload == "serving" else run_reference)(args, world, rank, local)
+            runner = {"serving": run_serving_reference, "rf2iq": run_frontend_reference,
+                      "ingest": run_frontend_reference}.get(args.workload, run_reference)
         else:
-            line = (run_serving if args.workload == "serving" else run_ours)(args, world, rank, local)
+            runner = {"serving": run_serving, "rf2iq": run_frontend, "ingest": run_frontend}.get(args.workload, run_ours)
+        line = runner(args, world, rank, local)
         if rank == 0:
             print(json.dumps(line), flush=True)
     finally:

@@ -178,6 +178,7 @@ cudaError_t launch_ingest(int src_code, const void* src, int dst_code, void* dst
 // element sum(c_i * src_stride[i]) + s * src_sample, and its complex result at
 // sum(c_i * dst_stride[i]) + s * dst_sample (in complex elements).
 constexpr int kHilMaxStages = 32;
+constexpr int kHilRoots = 256;  // shared-memory roots of the odd register radices (float2)
 struct HilbertArgs {
     const void* src;
     void* dst;
@@ -187,7 +188,9 @@ struct HilbertArgs {
     float inv_n;              // 1 / n
     float scale;              // both parts of the result are multiplied by it before rounding
     int64_t n_cols;
-    int cols_per_cta;         // even: columns are transformed in pairs
+    int cols_log2;            // 1..4: a CTA takes 2^cols_log2 columns, transformed in pairs
+    int pair_stride;          // float2 between the shared-memory buffers of two column pairs
+    int x_in_smem;            // 1: the group's samples are kept in shared memory for the output
     int load_cols_fast;       // 1: consecutive threads read consecutive columns of one sample
     int store_cols_fast;      // 1: consecutive threads write consecutive columns of one sample
     int64_t n0, n1;
@@ -197,14 +200,15 @@ struct HilbertArgs {
     int64_t dst_sample;
 };
 
-// Radices of the Stockham stages for length n (8, 4, 2 first, then odd primes); -1 if more
-// than max_stages.
+// Radices of the Stockham stages for length n (16, 8, 4, 2 first, then odd primes); -1 if
+// more than max_stages.
 int hilbert_plan(int n, int* radix, int max_stages);
 
 // Real storage src_code (kF32/kF16/kBF16/kI16) to complex dst_code (kC64/kCF16/kCBF16/kCI16);
-// `smem` = 8 n (cols_per_cta + 1) bytes.
-cudaError_t launch_hilbert(int src_code, int dst_code, const HilbertArgs& g, int blocks, size_t smem,
-                           cudaStream_t st);
+// `smem` = 8 (n + kHilRoots + 2^cols_log2 pair_stride) bytes (two buffers of pair_stride float2
+// per column pair), plus 4 n 2^cols_log2 with x_in_smem.  A persistent grid of at most the
+// resident CTAs.
+cudaError_t launch_hilbert(int src_code, int dst_code, const HilbertArgs& g, size_t smem, cudaStream_t st);
 
 // Power-Doppler epilogue (das_power.cu): out[v] (+)= sum over frames of |in[v][f]|^2.
 cudaError_t launch_power_epilogue(const void* in, float* out, int64_t n_vox, int n_frames, bool cplx, bool accumulate,

@@ -954,21 +954,32 @@ int hilbert_impl(int32_t src_storage, const void* src, int32_t src_layout, int32
     if (g.n_stages < 0) return fail(MACH_B200_ERR_VALUE, "n_samples %u has too many factors", n_samples);
     int device = 0;
     MACH_B200_CUDA_TRY(cudaGetDevice(&device));
-    int max_smem = 0, n_sm = 0;
+    int max_smem = 0;
     MACH_B200_CUDA_TRY(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
-    MACH_B200_CUDA_TRY(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, device));
-    // Shared memory: twiddle table + two buffers of one complex column per column pair.
-    const uint64_t col_bytes = 8ull * g.n;
-    const uint64_t two_per_sm = 113ull << 10;
-    if (col_bytes * 3 > static_cast<uint64_t>(max_smem)) {
+    // Shared memory: stage twiddles + odd-radix roots + two padded buffers per column pair.
+    g.pair_stride = g.n + (g.n >> 5) + 1;  // one float2 of padding per 32
+    const uint64_t col_bytes = 8ull * g.pair_stride;
+    const uint64_t fixed = 8ull * (kHilRoots + g.n);
+    if (col_bytes * 2 + fixed > static_cast<uint64_t>(max_smem)) {
         return fail(MACH_B200_ERR_VALUE, "n_samples %u is too long for the on-device analytic signal (at most %d)",
-                    n_samples, max_smem / 24);
+                    n_samples, static_cast<int>((max_smem - 8 * kHilRoots) / 24 * 32 / 33));
     }
+    int roots = 0;
+    for (int s = 0; s < g.n_stages; ++s) roots += (g.radix[s] & 1) && g.radix[s] <= 16 ? g.radix[s] : 0;
+    if (roots > kHilRoots) return fail(MACH_B200_ERR_VALUE, "n_samples %u has too many odd factors", n_samples);
     const int64_t n_cols = static_cast<int64_t>(n_elements) * n_waves * n_frames;
-    int cols = 2;
-    while (cols < 16 && col_bytes * (cols + 3) <= two_per_sm && cols < n_cols) cols += 2;
-    g.cols_per_cta = cols;
-    const size_t smem = static_cast<size_t>(col_bytes * (cols + 1));
+    // 2, 4, 8 or 16 columns per CTA: as many as keep two CTAs on an SM (113 KB each) with at
+    // most 8192 samples per group (32 per thread, prefetched into registers), plus the group's
+    // samples in shared memory (xs) for the output phase when they fit.
+    auto bytes_for = [&](int l, bool xs) { return col_bytes * (1ull << l) + fixed + (xs ? 4ull * g.n << l : 0); };
+    int lc = 1;
+    while (lc < 4 && bytes_for(lc + 1, true) <= (113ull << 10) && (static_cast<int64_t>(g.n) << (lc + 1)) <= 8192 &&
+           (int64_t{1} << lc) < n_cols) {
+        ++lc;
+    }
+    g.cols_log2 = lc;
+    g.x_in_smem = bytes_for(lc, true) <= static_cast<uint64_t>(max_smem) ? 1 : 0;
+    const size_t smem = static_cast<size_t>(bytes_for(lc, g.x_in_smem != 0));
     g.n_cols = n_cols;
     g.inv_n = 1.0f / static_cast<float>(g.n);
     g.scale = scale;
@@ -1008,11 +1019,8 @@ int hilbert_impl(int32_t src_storage, const void* src, int32_t src_layout, int32
         g.src = staged.ptr;
     }
     g.dst = dst;
-    const int64_t groups = (n_cols + cols - 1) / cols;
-    const int per_sm = std::max<int>(1, static_cast<int>(std::min<uint64_t>(2, (228ull << 10) / (smem + 1024))));
-    const int blocks = static_cast<int>(std::min<int64_t>(groups, static_cast<int64_t>(n_sm) * per_sm));
     g_launches.fetch_add(1, std::memory_order_relaxed);
-    MACH_B200_CUDA_TRY(launch_hilbert(src_storage, dst_storage, g, blocks, smem, stream));
+    MACH_B200_CUDA_TRY(launch_hilbert(src_storage, dst_storage, g, smem, stream));
     if (r_src != kOnDevice || !(flags & MACH_B200_FLAG_ASYNC)) MACH_B200_CUDA_TRY(cudaStreamSynchronize(stream));
     return MACH_B200_OK;
 }
