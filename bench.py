@@ -119,6 +119,8 @@ class ClockSampler:
         self.thread = None
 
     def start(self):
+        """Start sampling; returns once the first sample is in (at most 3 s), so that even a
+        short timed region is bracketed by samples."""
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
@@ -128,6 +130,9 @@ class ClockSampler:
             return
         self.thread = threading.Thread(target=self._read, daemon=True)
         self.thread.start()
+        t0 = time.perf_counter()
+        while not self.lines and time.perf_counter() - t0 < 3.0 and self.proc.poll() is None:
+            time.sleep(0.01)
 
     def _read(self):
         for line in self.proc.stdout:
@@ -136,6 +141,10 @@ class ClockSampler:
     def stop(self) -> dict:
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        seen = len(self.lines)  # one more sample after the timed region (at most 1 s)
+        t0 = time.perf_counter()
+        while len(self.lines) == seen and time.perf_counter() - t0 < 1.0 and self.proc.poll() is None:
+            time.sleep(0.01)
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
