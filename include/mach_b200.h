@@ -91,8 +91,9 @@ typedef struct mach_b200_options {
     int32_t window_rows;     /* staged / ensemble kernels: sample rows per window, 0 = automatic */
     int32_t lanes_per_voxel; /* staged kernel: 4, 8, 16 or 32, 0 = automatic */
     int32_t tx_model;        /* MACH_B200_TX_ARRAYS: read tx_wave_arrivals_s; MACH_B200_TX_PLANE /
-                                MACH_B200_TX_SPHERICAL: compute every (voxel, transmit) arrival on the
-                                device from tx_params (tx_wave_arrivals_s may then be NULL) */
+                                MACH_B200_TX_SPHERICAL: every (point, transmit) arrival is formed on the
+                                device from tx_params, by one kernel into a temporary [n_tx][n_scan]
+                                device array (tx_wave_arrivals_s may then be NULL) */
     int32_t reserved0;
     const double* tx_params; /* [n_tx][8]: origin xyz (m), unit direction (plane) or focus xyz (m)
                                 (spherical), time offset (s), unused.  The arrival is the distance of
@@ -175,6 +176,8 @@ MACH_B200_API int mach_b200_beamform_ex(int32_t storage, const void* channel_dat
  *   kernel (nearest or linear interpolation, 16-byte aligned channel_data, n_frames x sample
  *   bytes a multiple of 16, fewer than 2^31 voxels) and need at most 64 launches, i.e. at most
  *   64 x (2^31 - 1) channel samples; anything else is rejected with MACH_B200_ERR_VALUE.
+ *   It takes an arrivals array only: options->tx_model must be MACH_B200_TX_ARRAYS, since a
+ *   wave model is turned into arrivals in a device buffer.
  * - The first call on a device looks up the counters' device address; make that first call
  *   before any stream capture.
  * - All calls share the counters (each call zeroes the ones it uses on `cuda_stream`), so two

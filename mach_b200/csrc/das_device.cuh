@@ -130,12 +130,6 @@ struct DasArgs {
     // per (voxel, transmit), each split into an integer sample base + FP32 fraction.
     int32_t split;
     int32_t power;          // ensemble kernel: out is float [n_vox], += sum over frames of |x|^2
-    // Transmit arrivals: 0 = read `arrivals`; 1 = plane waves, 2 = spherical waves, computed
-    // per (voxel, transmit) from tx_params [n_tx][8] (FP64): origin xyz, direction or focus xyz,
-    // time offset (s).
-    int32_t tx_model;
-    const double* tx_params;
-    double sound_speed_d;
     int32_t start_base;     // floor(-t0 * fs): samples before it belong to tau < 0
     float start_frac;       // -t0 * fs - start_base
     double fs_d;            // sampling frequency
@@ -144,28 +138,6 @@ struct DasArgs {
     double fs_over_c;       // fs / c
     double fmod_over_c;     // f_mod / c
 };
-
-// Transmit arrival time of voxel v for transmit t: the `arrivals` array, or the plane /
-// spherical wave model evaluated in FP64 and rounded to FP32 (what the host path computes,
-// src/mach/wavefront.py:8-116 divided by the sound speed, then cast by src/mach/kernel.py:233).
-__device__ __forceinline__ float tx_arrival(const DasArgs& a, int t, int64_t v) {
-    if (a.tx_model == 0) return __ldg(a.arrivals + static_cast<int64_t>(t) * a.n_vox + v);
-    const double* q = a.tx_params + 8 * t;
-    const double px = __ldg(a.scan + 3 * v + 0), py = __ldg(a.scan + 3 * v + 1), pz = __ldg(a.scan + 3 * v + 2);
-    const double ox = __ldg(q + 0), oy = __ldg(q + 1), oz = __ldg(q + 2);
-    const double gx = __ldg(q + 3), gy = __ldg(q + 4), gz = __ldg(q + 5);
-    double d;
-    if (a.tx_model == 1) {  // plane: (p - o) . direction
-        d = (px - ox) * gx + (py - oy) * gy + (pz - oz) * gz;
-    } else {  // spherical: |o - f| sign(f_z - o_z) - |f - p| sign(f_z - p_z)
-        const double of = sqrt((ox - gx) * (ox - gx) + (oy - gy) * (oy - gy) + (oz - gz) * (oz - gz));
-        const double fp = sqrt((gx - px) * (gx - px) + (gy - py) * (gy - py) + (gz - pz) * (gz - pz));
-        const double so = gz > oz ? 1.0 : (gz < oz ? -1.0 : 0.0);
-        const double sp = gz > pz ? 1.0 : (gz < pz ? -1.0 : 0.0);
-        d = of * so - fp * sp;
-    }
-    return static_cast<float>(d / a.sound_speed_d + __ldg(q + 6));
-}
 
 // Integer base + FP32 fraction in [0, 1) of a non-negative-or-negative FP64 sample position.
 struct SplitPos {

@@ -304,7 +304,7 @@ __global__ void __launch_bounds__(kEnsThreads, 1)
         const float radius = __fdiv_rn(vz, a.two_f_number);  // kernel.cu:583
         const float radius_sq = __fmul_rn(radius, radius);
         for (int t = 0; t < n_pref; ++t) {
-            s.arr[t * kEnsTileVoxels + tt] = pv >= 0 ? tx_arrival(a, t, pv) : 0.f;
+            s.arr[t * kEnsTileVoxels + tt] = pv >= 0 ? __ldg(a.arrivals + static_cast<int64_t>(t) * a.n_vox + pv) : 0.f;
         }
         {
             float b[5] = {pv >= 0 ? vx : INFINITY, pv >= 0 ? -vx : INFINITY, pv >= 0 ? vy : INFINITY,
@@ -404,7 +404,7 @@ __global__ void __launch_bounds__(kEnsThreads, 1)
                 bool ok = false;
                 if (pair_ok) {
                     const float txa = n_pref ? s.arr[t * kEnsTileVoxels + tt]
-                                             : tx_arrival(a, t, pv);
+                                             : __ldg(a.arrivals + static_cast<int64_t>(t) * a.n_vox + pv);
                     TapPosition tp{};
                     float sn = 0.f, cs = 1.f;
                     if (SPLIT) {

@@ -79,7 +79,7 @@ __global__ void __launch_bounds__(kThreadsPerBlock) das_gather_kernel(const __gr
         float txa[kTxGroup];
 #pragma unroll
         for (int j = 0; j < kTxGroup; ++j) {
-            txa[j] = (vox_ok && tg + j < a.n_tx) ? tx_arrival(a, tg + j, v) : 0.f;
+            txa[j] = (vox_ok && tg + j < a.n_tx) ? __ldg(a.arrivals + static_cast<int64_t>(tg + j) * a.n_vox + v) : 0.f;
         }
 
         for (int eb = 0; eb < a.n_rx; eb += 32) {

@@ -255,7 +255,7 @@ __device__ __forceinline__ void lane_voxel_tile(const DasArgs& a, int64_t tile, 
         for (int i = threadIdx.x; i < nt * kLaneVoxelThreads; i += kLaneVoxelThreads) {
             const int t = i / kLaneVoxelThreads;
             const int64_t vv = tile * kLaneVoxelThreads + (i - t * kLaneVoxelThreads);
-            const float txa = vv < a.n_vox ? tx_arrival(a, t0 + t, vv) : 0.f;
+            const float txa = vv < a.n_vox ? __ldg(a.arrivals + static_cast<int64_t>(t0 + t) * a.n_vox + vv) : 0.f;
             if constexpr (SPLIT) {
                 // transmit part of the sample position and phase, per (voxel, transmit)
                 const SplitPos sp = split_position((static_cast<double>(txa) - a.t0_d) * a.fs_d);

@@ -210,6 +210,12 @@ int hilbert_plan(int n, int* radix, int max_stages);
 // resident CTAs.
 cudaError_t launch_hilbert(int src_code, int dst_code, const HilbertArgs& g, size_t smem, cudaStream_t st);
 
+// Transmit arrivals of a plane (model 1) or spherical (model 2) wave table (das_transmit.cu):
+// out[t][v] for t < n_tx, v < n_scan; params [n_tx][8] FP64, scan [n_scan][3] FP32, all
+// device memory.
+cudaError_t launch_tx_arrivals(int model, const double* params, const float* scan, int64_t n_scan, int n_tx,
+                               double sound_speed, float* out, cudaStream_t st);
+
 // Power-Doppler epilogue (das_power.cu): out[v] (+)= sum over frames of |in[v][f]|^2.
 cudaError_t launch_power_epilogue(const void* in, float* out, int64_t n_vox, int n_frames, bool cplx, bool accumulate,
                                   cudaStream_t stream);

@@ -263,7 +263,7 @@ __device__ __forceinline__ bool staged_tile(const DasArgs& a, const StagedArgs& 
     for (int i = tid; i < n_pref * kTileVoxels; i += kStagedThreads) {
         const int t = i / kTileVoxels;
         const int64_t vv = tile_voxel(a, st, tile, i - t * kTileVoxels);
-        s_arr[i] = vv >= 0 ? tx_arrival(a, t, vv) : 0.f;
+        s_arr[i] = vv >= 0 ? __ldg(a.arrivals + static_cast<int64_t>(t) * a.n_vox + vv) : 0.f;
     }
     {
         float b[5] = {pv >= 0 ? vx : INFINITY, pv >= 0 ? -vx : INFINITY, pv >= 0 ? vy : INFINITY,
@@ -371,7 +371,7 @@ __device__ __forceinline__ bool staged_tile(const DasArgs& a, const StagedArgs& 
             bool ok = false;
             if (pair_ok) {
                 const float txa = n_pref ? s_arr[t * kTileVoxels + tid]
-                                         : tx_arrival(a, t, pv);
+                                         : __ldg(a.arrivals + static_cast<int64_t>(t) * a.n_vox + pv);
                 TapPosition tp{};
                 float sn = 0.f, cs = 1.f;
                 if (a.split) {

@@ -452,8 +452,7 @@ int dispatch_split(int storage, DasArgs a, int interp, const Plan& plan, cudaStr
         DasArgs b = a;
         b.n_tx = static_cast<int32_t>(std::min<int64_t>(max_tx, total - t0));
         b.channel = ch + static_cast<size_t>(t0) * per_tx * esz;
-        b.arrivals = arr ? arr + static_cast<int64_t>(t0) * a.n_vox : nullptr;
-        b.tx_params = a.tx_params ? a.tx_params + 8 * static_cast<int64_t>(t0) : nullptr;
+        b.arrivals = arr + static_cast<int64_t>(t0) * a.n_vox;
         b.accumulate = t0 == 0 ? a.accumulate : 1;
         CUtensorMap map;
         std::memset(&map, 0, sizeof(map));
@@ -575,40 +574,6 @@ int check_args(int32_t storage, int32_t interp_type, float tukey_alpha, uint32_t
     return MACH_B200_OK;
 }
 
-// Transmit model of a call: checks, and the device copy of host parameters.  `arrivals_ok`
-// tells whether tx_wave_arrivals_s is needed (model 0) or ignored.
-struct TxModel {
-    int model = 0;
-    const double* params = nullptr;  // device memory
-    DeviceBuffer staged;
-};
-
-int setup_tx_model(const mach_b200_options& o, uint32_t n_tx, int device, cudaStream_t stream, TxModel& tm) {
-    tm.model = o.tx_model;
-    if (tm.model == MACH_B200_TX_ARRAYS) return MACH_B200_OK;
-    if (tm.model != MACH_B200_TX_PLANE && tm.model != MACH_B200_TX_SPHERICAL) {
-        return fail(MACH_B200_ERR_VALUE, "tx_model must be 0 (arrays), 1 (plane) or 2 (spherical), got %d", tm.model);
-    }
-    if (!o.tx_params) return fail(MACH_B200_ERR_VALUE, "tx_model %d needs tx_params", tm.model);
-    Residency r;
-    int rc;
-    if ((rc = residency(o.tx_params, device, &r, "tx_params"))) return rc;
-    tm.params = o.tx_params;
-    if (r != kOnDevice && n_tx > 0) {
-        const size_t bytes = static_cast<size_t>(n_tx) * 8 * sizeof(double);
-        MACH_B200_CUDA_TRY(tm.staged.alloc(bytes, stream));
-        MACH_B200_CUDA_TRY(cudaMemcpyAsync(tm.staged.ptr, o.tx_params, bytes, cudaMemcpyHostToDevice, stream));
-        tm.params = static_cast<const double*>(tm.staged.ptr);
-    }
-    return MACH_B200_OK;
-}
-
-void apply_tx_model(DasArgs& a, const TxModel& tm, float sound_speed_m_s) {
-    a.tx_model = tm.model;
-    a.tx_params = tm.params;
-    a.sound_speed_d = sound_speed_m_s;
-}
-
 int power_impl(int32_t storage, const void* channel_data, const float* rx_coords_m, const float* scan_coords_m,
                const float* tx_wave_arrivals_s, void* out, uint32_t n_tx, uint32_t n_rx, uint32_t n_samples,
                uint64_t n_scan, uint32_t n_frames, float f_number, float rx_start_s, float sampling_freq_hz,
@@ -632,8 +597,7 @@ int compound_impl(int32_t storage, const void* channel_data, const float* rx_coo
     if (n_scan == 0 || n_frames == 0) return MACH_B200_OK;  // empty output: nothing to write
     if (!out || !scan_coords_m) return fail(MACH_B200_ERR_VALUE, "out and scan_coords_m must not be NULL");
     const bool need_channel = n_tx > 0 && n_rx > 0 && n_samples > 0;
-    const bool need_arrivals = opt.tx_model == MACH_B200_TX_ARRAYS;
-    if (need_channel && (!channel_data || !rx_coords_m || (need_arrivals && !tx_wave_arrivals_s))) {
+    if (need_channel && (!channel_data || !rx_coords_m || !tx_wave_arrivals_s)) {
         return fail(MACH_B200_ERR_VALUE, "channel_data, rx_coords_m and tx_wave_arrivals_s must not be NULL");
     }
 
@@ -642,13 +606,11 @@ int compound_impl(int32_t storage, const void* channel_data, const float* rx_coo
     DeviceState* dev = nullptr;
     int rc;
     if ((rc = device_state(device, &dev))) return rc;
-    TxModel tm;
-    if ((rc = setup_tx_model(opt, n_tx, device, stream, tm))) return rc;
     Residency r_ch = kOnDevice, r_rx = kOnDevice, r_scan = kOnDevice, r_arr = kOnDevice, r_out = kOnDevice;
     if (need_channel) {
         if ((rc = residency(channel_data, device, &r_ch, "channel_data"))) return rc;
         if ((rc = residency(rx_coords_m, device, &r_rx, "rx_coords_m"))) return rc;
-        if (need_arrivals && (rc = residency(tx_wave_arrivals_s, device, &r_arr, "tx_wave_arrivals_s"))) return rc;
+        if ((rc = residency(tx_wave_arrivals_s, device, &r_arr, "tx_wave_arrivals_s"))) return rc;
     }
     if ((rc = residency(scan_coords_m, device, &r_scan, "scan_coords_m"))) return rc;
     if ((rc = residency(out, device, &r_out, "out"))) return rc;
@@ -660,7 +622,6 @@ int compound_impl(int32_t storage, const void* channel_data, const float* rx_coo
     DasArgs a = make_args(rx_coords_m, scan_coords_m, n_scan, need_channel ? n_rx : 0, n_samples, n_frames, f_number,
                           rx_start_s, sampling_freq_hz, sound_speed_m_s, modulation_freq_hz, tukey_alpha,
                           channel_scale, cplx, flags);
-    apply_tx_model(a, tm, sound_speed_m_s);
     const bool overwrite = (flags & MACH_B200_FLAG_OVERWRITE) != 0u || r_out != kOnDevice;
     Plan plan = plan_launch(storage, n_scan, n_frames, n_tx, channel_data, r_ch == kOnDevice, opt, interp_type);
     plan.st.status = dev->status;
@@ -756,9 +717,8 @@ int compound_impl(int32_t storage, const void* channel_data, const float* rx_coo
                                                    cudaMemcpyHostToDevice, copy.s));
                 a.arrivals = static_cast<const float*>(d_arr[b].ptr);
             } else {
-                a.arrivals = h_arr ? reinterpret_cast<const float*>(h_arr + arr_bytes * t0) : nullptr;
+                a.arrivals = reinterpret_cast<const float*>(h_arr + arr_bytes * t0);
             }
-            a.tx_params = tm.params ? tm.params + 8 * static_cast<size_t>(t0) : nullptr;
             MACH_B200_CUDA_TRY(cudaEventRecord(copied.ev[b], copy.s));
             MACH_B200_CUDA_TRY(cudaStreamWaitEvent(stream, copied.ev[b], 0));
             a.n_tx = static_cast<int32_t>(nt);
@@ -773,6 +733,54 @@ int compound_impl(int32_t storage, const void* channel_data, const float* rx_coo
     // Host buffers are in use until the stream drains: always synchronous here.
     MACH_B200_CUDA_TRY(cudaStreamSynchronize(stream));
     if (plan.staged || plan.ensemble) return check_status(dev, stream);
+    return MACH_B200_OK;
+}
+
+// ---------------------------------------------------------------- transmit models
+//
+// mach_b200_options.tx_model != 0: the [n_tx][n_scan] arrivals are formed on the device by one
+// kernel (das_transmit.cu) from the FP64 table tx_params, and the call then runs as with an
+// arrivals array.  Only the table and, for host scan points, the points cross the host link.
+
+struct TxArrivals {
+    DeviceBuffer params, scan, arr;
+    const float* ptr = nullptr;
+};
+
+int form_tx_arrivals(const mach_b200_options& o, const float* scan_coords_m, uint32_t n_tx, uint64_t n_scan,
+                     float sound_speed_m_s, cudaStream_t stream, TxArrivals& t) {
+    if (o.tx_model != MACH_B200_TX_PLANE && o.tx_model != MACH_B200_TX_SPHERICAL) {
+        return fail(MACH_B200_ERR_VALUE, "tx_model must be 0 (arrays), 1 (plane) or 2 (spherical), got %d", o.tx_model);
+    }
+    if (!o.tx_params) return fail(MACH_B200_ERR_VALUE, "tx_model %d needs tx_params", o.tx_model);
+    if (n_tx == 0 || n_scan == 0) return MACH_B200_OK;
+    if (!scan_coords_m) return fail(MACH_B200_ERR_VALUE, "out and scan_coords_m must not be NULL");
+    int device = 0;
+    MACH_B200_CUDA_TRY(cudaGetDevice(&device));
+    Residency r_p, r_s;
+    int rc;
+    if ((rc = residency(o.tx_params, device, &r_p, "tx_params"))) return rc;
+    if ((rc = residency(scan_coords_m, device, &r_s, "scan_coords_m"))) return rc;
+    const double* params = o.tx_params;
+    if (r_p != kOnDevice) {
+        const size_t bytes = static_cast<size_t>(n_tx) * 8 * sizeof(double);
+        MACH_B200_CUDA_TRY(t.params.alloc(bytes, stream));
+        MACH_B200_CUDA_TRY(cudaMemcpyAsync(t.params.ptr, o.tx_params, bytes, cudaMemcpyHostToDevice, stream));
+        params = static_cast<const double*>(t.params.ptr);
+    }
+    const float* scan = scan_coords_m;
+    if (r_s != kOnDevice) {
+        const size_t bytes = static_cast<size_t>(n_scan) * 12;
+        MACH_B200_CUDA_TRY(t.scan.alloc(bytes, stream));
+        MACH_B200_CUDA_TRY(cudaMemcpyAsync(t.scan.ptr, scan_coords_m, bytes, cudaMemcpyHostToDevice, stream));
+        scan = static_cast<const float*>(t.scan.ptr);
+    }
+    MACH_B200_CUDA_TRY(t.arr.alloc(static_cast<size_t>(n_tx) * n_scan * sizeof(float), stream));
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    MACH_B200_CUDA_TRY(launch_tx_arrivals(o.tx_model, params, scan, static_cast<int64_t>(n_scan),
+                                          static_cast<int>(n_tx), static_cast<double>(sound_speed_m_s),
+                                          static_cast<float*>(t.arr.ptr), stream));
+    t.ptr = static_cast<const float*>(t.arr.ptr);
     return MACH_B200_OK;
 }
 
@@ -804,8 +812,7 @@ int power_impl(int32_t storage, const void* channel_data, const float* rx_coords
     if (n_scan == 0) return MACH_B200_OK;
     if (!out || !scan_coords_m) return fail(MACH_B200_ERR_VALUE, "out and scan_coords_m must not be NULL");
     const bool need_channel = n_tx > 0 && n_rx > 0 && n_samples > 0 && n_frames > 0;
-    const bool need_arrivals = opt.tx_model == MACH_B200_TX_ARRAYS;
-    if (need_channel && (!channel_data || !rx_coords_m || (need_arrivals && !tx_wave_arrivals_s))) {
+    if (need_channel && (!channel_data || !rx_coords_m || !tx_wave_arrivals_s)) {
         return fail(MACH_B200_ERR_VALUE, "channel_data, rx_coords_m and tx_wave_arrivals_s must not be NULL");
     }
     int device = 0;
@@ -818,7 +825,7 @@ int power_impl(int32_t storage, const void* channel_data, const float* rx_coords
     if (need_channel) {
         const void* ptrs[4] = {channel_data, rx_coords_m, scan_coords_m, tx_wave_arrivals_s};
         const char* names[4] = {"channel_data", "rx_coords_m", "scan_coords_m", "tx_wave_arrivals_s"};
-        for (int i = 0; i < (need_arrivals ? 4 : 3); ++i) {
+        for (int i = 0; i < 4; ++i) {
             Residency r;
             if ((rc = residency(ptrs[i], device, &r, names[i]))) return rc;
             all_device = all_device && r == kOnDevice;
@@ -837,9 +844,6 @@ int power_impl(int32_t storage, const void* channel_data, const float* rx_coords
             DasArgs a = make_args(rx_coords_m, scan_coords_m, n_scan, n_rx, n_samples, n_frames, f_number, rx_start_s,
                                   sampling_freq_hz, sound_speed_m_s, modulation_freq_hz, tukey_alpha, channel_scale,
                                   cplx, flags);
-            TxModel tm;
-            if ((rc = setup_tx_model(opt, n_tx, device, stream, tm))) return rc;
-            apply_tx_model(a, tm, sound_speed_m_s);
             a.frame_passes = plan.lp.passes;
             a.tx_chunk = plan.lp.tx_chunk;
             a.channel = channel_data;
@@ -1070,27 +1074,19 @@ int noalloc_impl(int32_t storage, const void* channel_data, const float* rx_coor
     if (n_scan == 0 || n_frames == 0) return MACH_B200_OK;
     if (!out || !scan_coords_m) return fail(MACH_B200_ERR_VALUE, "out and scan_coords_m must not be NULL");
     const bool need_channel = n_tx > 0 && n_rx > 0 && n_samples > 0;
-    const bool need_arrivals = opt.tx_model == MACH_B200_TX_ARRAYS;
-    if (need_channel && (!channel_data || !rx_coords_m || (need_arrivals && !tx_wave_arrivals_s))) {
+    if (need_channel && (!channel_data || !rx_coords_m || !tx_wave_arrivals_s)) {
         return fail(MACH_B200_ERR_VALUE, "channel_data, rx_coords_m and tx_wave_arrivals_s must not be NULL");
     }
     int device = 0;
     MACH_B200_CUDA_TRY(cudaGetDevice(&device));
     DeviceState* dev = nullptr;
     if ((rc = device_state(device, &dev))) return rc;
-    TxModel tm;
-    if (!need_arrivals) {
-        Residency rp = kOnDevice;
-        if (opt.tx_params && (rc = residency(opt.tx_params, device, &rp, "tx_params"))) return rc;
-        if (rp != kOnDevice) return fail(MACH_B200_ERR_VALUE, "tx_params must be device memory for this call");
-        if ((rc = setup_tx_model(opt, n_tx, device, stream, tm))) return rc;  // device params: nothing to copy
-    }
     int* counters = nullptr;
     if ((rc = noalloc_counters(device, &counters))) return rc;
     const void* ptrs[5] = {channel_data, rx_coords_m, scan_coords_m, tx_wave_arrivals_s, out};
     const char* names[5] = {"channel_data", "rx_coords_m", "scan_coords_m", "tx_wave_arrivals_s", "out"};
     for (int i = 0; i < 5; ++i) {
-        if (!ptrs[i] || (i == 3 && !need_arrivals)) continue;  // only optional inputs can be NULL here
+        if (!ptrs[i]) continue;  // only optional inputs can be NULL here (checked above)
         Residency r;
         if ((rc = residency(ptrs[i], device, &r, names[i]))) return rc;
         if (r != kOnDevice) {
@@ -1110,11 +1106,10 @@ int noalloc_impl(int32_t storage, const void* channel_data, const float* rx_coor
     DasArgs a = make_args(rx_coords_m, scan_coords_m, n_scan, need_channel ? n_rx : 0, n_samples, n_frames, f_number,
                           rx_start_s, sampling_freq_hz, sound_speed_m_s, modulation_freq_hz, tukey_alpha,
                           channel_scale, cplx, flags);
-    apply_tx_model(a, tm, sound_speed_m_s);
     a.frame_passes = plan.lp.passes;
     a.tx_chunk = plan.lp.tx_chunk;
     a.channel = channel_data;
-    a.arrivals = need_arrivals ? tx_wave_arrivals_s : nullptr;
+    a.arrivals = tx_wave_arrivals_s;
     a.out = out;
     a.n_tx = static_cast<int32_t>(need_channel ? n_tx : 0);
     a.accumulate = (flags & MACH_B200_FLAG_OVERWRITE) ? 0 : 1;
@@ -1139,8 +1134,7 @@ int noalloc_impl(int32_t storage, const void* channel_data, const float* rx_coor
         DasArgs b = a;
         b.n_tx = static_cast<int32_t>(std::min<int64_t>(max_tx, total - t0));
         b.channel = ch + static_cast<size_t>(t0) * per_tx * esz;
-        b.arrivals = a.arrivals ? a.arrivals + static_cast<int64_t>(t0) * a.n_vox : nullptr;
-        b.tx_params = a.tx_params ? a.tx_params + 8 * static_cast<int64_t>(t0) : nullptr;
+        b.arrivals = a.arrivals + static_cast<int64_t>(t0) * a.n_vox;
         b.accumulate = t0 == 0 ? a.accumulate : 1;
         CUtensorMap map;
         std::memset(&map, 0, sizeof(map));
@@ -1452,6 +1446,21 @@ int mach_b200_beamform_ex(int32_t storage, const void* channel_data, const float
         }
         std::memcpy(&o, options, std::min<size_t>(sizeof(o), options->struct_size));
     }
+    if (o.tx_model != MACH_B200_TX_ARRAYS) {
+        g_error.clear();
+        const int rc0 = check_args(storage, interp_type, tukey_alpha, n_tx, n_rx, n_samples, n_scan, n_frames);
+        if (rc0) return rc0;
+        TxArrivals t;  // freed in stream order when the call returns
+        const int rc = form_tx_arrivals(o, scan_coords_m, n_tx, n_scan, sound_speed_m_s,
+                                        static_cast<cudaStream_t>(cuda_stream), t);
+        if (rc) return rc;
+        o.tx_model = MACH_B200_TX_ARRAYS;
+        tx_wave_arrivals_s = t.ptr;
+        return compound_impl(storage, channel_data, rx_coords_m, scan_coords_m, tx_wave_arrivals_s, out, n_tx, n_rx,
+                             n_samples, n_scan, n_frames, f_number, rx_start_s, sampling_freq_hz, sound_speed_m_s,
+                             modulation_freq_hz, tukey_alpha, interp_type, channel_scale,
+                             static_cast<cudaStream_t>(cuda_stream), o);
+    }
     return compound_impl(storage, channel_data, rx_coords_m, scan_coords_m, tx_wave_arrivals_s, out, n_tx, n_rx,
                          n_samples, n_scan, n_frames, f_number, rx_start_s, sampling_freq_hz, sound_speed_m_s,
                          modulation_freq_hz, tukey_alpha, interp_type, channel_scale,
@@ -1472,6 +1481,11 @@ int mach_b200_beamform_ensemble_noalloc(int32_t storage, const void* channel_dat
             return MACH_B200_ERR_VALUE;
         }
         std::memcpy(&o, options, std::min<size_t>(sizeof(o), options->struct_size));
+    }
+    if (o.tx_model != MACH_B200_TX_ARRAYS) {
+        g_error = "mach_b200_beamform_ensemble_noalloc takes an arrivals array (tx_model 0): a wave model would "
+                  "need a device buffer for the arrivals";
+        return MACH_B200_ERR_VALUE;
     }
     return noalloc_impl(storage, channel_data, rx_coords_m, scan_coords_m, tx_wave_arrivals_s, out, n_tx, n_rx,
                         n_samples, n_scan, n_frames, f_number, rx_start_s, sampling_freq_hz, sound_speed_m_s,

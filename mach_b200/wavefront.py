@@ -47,11 +47,11 @@ class TransmitWaves:
 
     Pass an instance as ``tx_wave_arrivals_s`` of :func:`mach_b200.experimental.beamform`
     (or :func:`mach_b200.doppler.power_doppler`) instead of the ``[n_transmits, n_points]``
-    arrivals array: each (point, transmit) arrival is then computed inside the kernel from
-    the wave's origin and direction or focus, in FP64 and rounded to FP32, the same as
+    arrivals array: each (point, transmit) arrival is then computed on the GPU from the
+    wave's origin and direction or focus, in FP64 and rounded to FP32, the same as
     ``plane(...) / sound_speed`` or ``spherical(...) / sound_speed`` evaluated on the host.
-    The array (4 bytes per point and transmit, 79 MB for 75 transmits on 512x512) is never
-    formed, copied or read.
+    The array (4 bytes per point and transmit, 79 MB for 75 transmits on 512x512) is formed
+    in device memory and never crosses the host link.
     """
 
     model = 0

@@ -113,3 +113,7 @@ def test_noalloc_rejects_what_it_cannot_run(cuda):
     host_out = torch.zeros((w.n_vox, 64), dtype=torch.complex64)
     assert _call(fn, "c64", w, t, p, scale, host_out, opts) == 1
     assert b"device memory" in lib.mach_b200_last_error()
+    opts.tx_model = 1  # a wave model needs a device buffer for its arrivals
+    out = torch.zeros((w.n_vox, 64), dtype=torch.complex64, device="cuda")
+    assert _call(fn, "c64", w, t, p, scale, out, opts) == 1
+    assert b"tx_model 0" in lib.mach_b200_last_error()
