@@ -76,6 +76,7 @@ def parse_args():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--frames", type=int, default=None, help="override the workload's frame count (profiling)")
+    p.add_argument("--side", type=int, default=None, help="override the 3-D grid side (profiling)")
     return p.parse_args()
 
 
@@ -190,13 +191,14 @@ def profiled_traffic(key: str):
 # ----------------------------------------------------------------------------- workloads
 
 
-def make_workload(name: str, frames: int | None = None):
+def make_workload(name: str, frames: int | None = None, side: int | None = None):
     from mach_b200 import workloads as W
 
+    grid = {"n_side": side} if side else {}
     if name == "volume3d":
-        w = W.volume3d(n_frames=frames or 1, device="cuda")
+        w = W.volume3d(n_frames=frames or 1, device="cuda", **grid)
     elif name == "volume3d16":
-        w = W.volume3d(n_frames=frames or 16, device="cuda")
+        w = W.volume3d(n_frames=frames or 16, device="cuda", **grid)
     elif name == "doppler" and frames:
         w = W.doppler(n_frames=frames, device="cuda")
     else:
@@ -228,7 +230,7 @@ def algorithmic_bytes(w, storage) -> int:
 def run_ours(args, world, rank, local):
     from mach_b200 import _cuda_impl, _dlpack, experimental
 
-    w = make_workload(args.workload, args.frames)
+    w = make_workload(args.workload, args.frames, args.side)
     storage = args.storage or w.storage
     ch = storage_channel(w, storage)
     dev = torch.device("cuda", local)
@@ -800,7 +802,7 @@ def run_reference(args, world, rank, local):
             "warmup": args.warmup, "higher_is_better": True}
     if not machref.available():
         return {"impl": "reference", "unavailable": "mach's kernel was not built into oracle/_ref (no reference checkout)"}
-    w = make_workload(args.workload, args.frames)
+    w = make_workload(args.workload, args.frames, args.side)
     ch = w.channel
     if ch.dtype == torch.int16:
         ch = ch.to(torch.float32) * w.channel_scale
