@@ -130,6 +130,10 @@ struct DasArgs {
     // per (voxel, transmit), each split into an integer sample base + FP32 fraction.
     int32_t split;
     int32_t power;          // ensemble kernel: out is float [n_vox], += sum over frames of |x|^2
+    // Lane-voxel kernels on a known grid: map_fast = voxels along the contiguous axis,
+    // map_outer = n_vox / map_fast; 0 = tiles of 128 consecutive voxels.
+    int32_t map_fast;
+    int64_t map_outer;
     int32_t start_base;     // floor(-t0 * fs): samples before it belong to tau < 0
     float start_frac;       // -t0 * fs - start_base
     double fs_d;            // sampling frequency

@@ -196,6 +196,19 @@ __device__ __forceinline__ float fast_tukey(float h2, float radius, const DasArg
     return __fmaf_rn(-0.5f, __cosf(__fdividef(kPi * (1.0f - r), a.alpha)), 0.5f);
 }
 
+// Voxel of thread j (0..127) of lane-voxel tile `tile`, or n_vox for none.  On a known grid a
+// warp takes 4 neighbours along the contiguous axis times 8 along the next one (a CTA 4 x 32),
+// so that the sample rows the 32 lanes of a load read lie close together in memory (few L1
+// lines per warp load); otherwise a tile is 128 consecutive voxels.
+__device__ __forceinline__ int64_t lane_voxel_index(const DasArgs& a, int64_t tile, int j) {
+    if (a.map_fast <= 0) return tile * kLaneVoxelThreads + j;
+    const int64_t tiles_fast = (a.map_fast + 3) >> 2;
+    const int64_t to = tile / tiles_fast;
+    const int64_t o = to * 32 + (j >> 2);
+    const int64_t f = (tile - to * tiles_fast) * 4 + (j & 3);
+    return (o < a.map_outer && f < a.map_fast) ? o * a.map_fast + f : a.n_vox;
+}
+
 // One CTA tile: voxels [tile * 128, tile * 128 + 128) of job `a`, all its transmits,
 // elements and frames.  `smem_words` is the dynamic shared memory (tx_chunk x 128 words,
 // x3 in split mode).  Shared by the per-job kernel and the persistent batch kernel.
@@ -211,7 +224,7 @@ __device__ __forceinline__ void lane_voxel_tile(const DasArgs& a, int64_t tile, 
     float* const s_cyc = s_arrival + 2 * a.tx_chunk * kLaneVoxelThreads;
 
     const int lane = threadIdx.x & 31;
-    const int64_t v = tile * kLaneVoxelThreads + threadIdx.x;
+    const int64_t v = lane_voxel_index(a, tile, threadIdx.x);
     const bool vox_ok = v < a.n_vox;
     const int n_frames = NF > 0 ? NF : a.n_frames;
 
@@ -253,9 +266,8 @@ __device__ __forceinline__ void lane_voxel_tile(const DasArgs& a, int64_t tile, 
         const int nt = min(tx_chunk, a.n_tx - t0);
         __syncthreads();
         for (int i = threadIdx.x; i < nt * kLaneVoxelThreads; i += kLaneVoxelThreads) {
-            const int t = i / kLaneVoxelThreads;
-            const int64_t vv = tile * kLaneVoxelThreads + (i - t * kLaneVoxelThreads);
-            const float txa = vv < a.n_vox ? __ldg(a.arrivals + static_cast<int64_t>(t0 + t) * a.n_vox + vv) : 0.f;
+            const int t = i / kLaneVoxelThreads;  // i - t * 128 is this thread's index: its own voxel
+            const float txa = vox_ok ? __ldg(a.arrivals + static_cast<int64_t>(t0 + t) * a.n_vox + v) : 0.f;
             if constexpr (SPLIT) {
                 // transmit part of the sample position and phase, per (voxel, transmit)
                 const SplitPos sp = split_position((static_cast<double>(txa) - a.t0_d) * a.fs_d);

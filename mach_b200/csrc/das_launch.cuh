@@ -29,6 +29,8 @@ struct LaunchPlan {
     dim3 grid;
     dim3 block;
     size_t smem;
+    int map_fast;       // lane-voxel kernels: grid tiling (DasArgs::map_fast), 0 = linear tiles
+    int64_t map_outer;
 };
 
 // Opt a kernel into more than 48 KB of dynamic shared memory (once per instance is enough,

@@ -298,6 +298,12 @@ Plan plan_launch(int storage, uint64_t n_vox, uint32_t n_frames, uint32_t n_tx, 
         p.lp.tx_chunk = static_cast<int>(std::max<uint32_t>(1u, (n_tx + chunks - 1) / chunks));
         p.lp.block = dim3(kLaneVoxelThreads, 1, 1);
         p.lp.grid = dim3(static_cast<unsigned>((n_vox + kLaneVoxelThreads - 1) / kLaneVoxelThreads), 1, 1);
+        if (grid_matches(o, n_vox) && o.grid_shape[2] >= 4) {  // 4 x 32 voxel tiles of the grid
+            p.lp.map_fast = o.grid_shape[2];
+            p.lp.map_outer = static_cast<int64_t>(n_vox / static_cast<uint64_t>(o.grid_shape[2]));
+            const int64_t tiles = ((p.lp.map_outer + 31) / 32) * ((p.lp.map_fast + 3) / 4);
+            p.lp.grid = dim3(static_cast<unsigned>(tiles), 1, 1);
+        }
         // split mode stages three words per (transmit, voxel): base, fraction, phase cycles
         p.lp.smem = static_cast<size_t>(p.lp.tx_chunk) * kLaneVoxelThreads * sizeof(float) *
                     ((o.flags & MACH_B200_FLAG_SPLIT_DELAY) ? 3 : 1);
@@ -627,6 +633,8 @@ int compound_impl(int32_t storage, const void* channel_data, const float* rx_coo
     plan.st.status = dev->status;
     a.frame_passes = plan.lp.passes;
     a.tx_chunk = plan.lp.tx_chunk;
+    a.map_fast = plan.lp.map_fast;
+    a.map_outer = plan.lp.map_outer;
 
     const bool all_device = r_ch == kOnDevice && r_rx == kOnDevice && r_scan == kOnDevice && r_arr == kOnDevice &&
                             r_out == kOnDevice;
@@ -1344,6 +1352,8 @@ int batch_run(mach_b200_batch* b, const mach_b200_job* jobs, uint32_t n_jobs, cu
         const Plan& p = plans[i];
         bj.a.frame_passes = p.lp.passes;
         bj.a.tx_chunk = p.lp.tx_chunk;
+        bj.a.map_fast = p.lp.map_fast;
+        bj.a.map_outer = p.lp.map_outer;
         bj.st = p.st;
         bj.st.status = dev->status;
         bj.tiles = static_cast<int32_t>(p.lp.grid.x);
