@@ -55,7 +55,7 @@ class Options(ctypes.Structure):
         ("window_rows", ctypes.c_int32),
         ("lanes_per_voxel", ctypes.c_int32),
         ("tx_model", ctypes.c_int32),
-        ("reserved0", ctypes.c_int32),
+        ("tile_fast", ctypes.c_int32),
         ("tx_params", ctypes.c_void_p),
     ]
 
@@ -64,7 +64,7 @@ KERNELS = {"auto": 0, "lane_voxel": 1, "staged": 2, "warp": 3, "ensemble": 4}
 
 
 def make_options(flags: int = 0, grid_shape=None, kernel: str | int = 0, tx_chunk: int = 0, window_rows: int = 0,
-                 lanes_per_voxel: int = 0) -> Options:
+                 lanes_per_voxel: int = 0, tile_fast: int = 0) -> Options:
     o = Options()
     o.struct_size = ctypes.sizeof(Options)
     o.flags = int(flags)
@@ -75,6 +75,7 @@ def make_options(flags: int = 0, grid_shape=None, kernel: str | int = 0, tx_chun
     o.tx_chunk = int(tx_chunk)
     o.window_rows = int(window_rows)
     o.lanes_per_voxel = int(lanes_per_voxel)
+    o.tile_fast = int(tile_fast)
     return o
 
 

@@ -131,8 +131,10 @@ struct DasArgs {
     int32_t split;
     int32_t power;          // ensemble kernel: out is float [n_vox], += sum over frames of |x|^2
     // Lane-voxel kernels on a known grid: map_fast = voxels along the contiguous axis,
-    // map_outer = n_vox / map_fast; 0 = tiles of 128 consecutive voxels.
+    // map_outer = n_vox / map_fast, a warp takes 2^map_wlog of them along the contiguous axis;
+    // map_fast = 0: tiles of 128 consecutive voxels.
     int32_t map_fast;
+    int32_t map_wlog;
     int64_t map_outer;
     int32_t start_base;     // floor(-t0 * fs): samples before it belong to tau < 0
     float start_frac;       // -t0 * fs - start_base

@@ -197,15 +197,16 @@ __device__ __forceinline__ float fast_tukey(float h2, float radius, const DasArg
 }
 
 // Voxel of thread j (0..127) of lane-voxel tile `tile`, or n_vox for none.  On a known grid a
-// warp takes 4 neighbours along the contiguous axis times 8 along the next one (a CTA 4 x 32),
-// so that the sample rows the 32 lanes of a load read lie close together in memory (few L1
-// lines per warp load); otherwise a tile is 128 consecutive voxels.
+// warp takes wf = 2^map_wlog neighbours along the contiguous axis times 32 / wf along the next
+// one (a CTA wf x 128 / wf), so that the sample rows the 32 lanes of a load read lie close
+// together in memory (few L1 lines per warp load); otherwise a tile is 128 consecutive voxels.
 __device__ __forceinline__ int64_t lane_voxel_index(const DasArgs& a, int64_t tile, int j) {
     if (a.map_fast <= 0) return tile * kLaneVoxelThreads + j;
-    const int64_t tiles_fast = (a.map_fast + 3) >> 2;
+    const int lw = a.map_wlog;
+    const int64_t tiles_fast = (a.map_fast + (1 << lw) - 1) >> lw;
     const int64_t to = tile / tiles_fast;
-    const int64_t o = to * 32 + (j >> 2);
-    const int64_t f = (tile - to * tiles_fast) * 4 + (j & 3);
+    const int64_t o = to * (kLaneVoxelThreads >> lw) + (j >> lw);
+    const int64_t f = ((tile - to * tiles_fast) << lw) + (j & ((1 << lw) - 1));
     return (o < a.map_outer && f < a.map_fast) ? o * a.map_fast + f : a.n_vox;
 }
 

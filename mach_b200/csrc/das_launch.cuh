@@ -29,7 +29,8 @@ struct LaunchPlan {
     dim3 grid;
     dim3 block;
     size_t smem;
-    int map_fast;       // lane-voxel kernels: grid tiling (DasArgs::map_fast), 0 = linear tiles
+    int map_fast;       // lane-voxel kernels: grid tiling (DasArgs::map_*), 0 = linear tiles
+    int map_wlog;
     int64_t map_outer;
 };
 

@@ -298,10 +298,18 @@ Plan plan_launch(int storage, uint64_t n_vox, uint32_t n_frames, uint32_t n_tx, 
         p.lp.tx_chunk = static_cast<int>(std::max<uint32_t>(1u, (n_tx + chunks - 1) / chunks));
         p.lp.block = dim3(kLaneVoxelThreads, 1, 1);
         p.lp.grid = dim3(static_cast<unsigned>((n_vox + kLaneVoxelThreads - 1) / kLaneVoxelThreads), 1, 1);
-        if (grid_matches(o, n_vox) && o.grid_shape[2] >= 4) {  // 4 x 32 voxel tiles of the grid
+        // On a known grid: CTA tiles of wf x (128 / wf) voxels, warps of wf x (32 / wf).
+        // Automatic: 2 along the contiguous axis for 16 frames (rows of 32+ bytes), else 4.
+        const int wf = o.tile_fast == 2 || o.tile_fast == 4 || o.tile_fast == 8 || o.tile_fast == 16
+                           ? o.tile_fast
+                           : (n_frames >= 16 ? 2 : 4);
+        if (grid_matches(o, n_vox) && o.grid_shape[2] >= wf) {
+            const int lw = wf == 2 ? 1 : (wf == 4 ? 2 : (wf == 8 ? 3 : 4));
             p.lp.map_fast = o.grid_shape[2];
+            p.lp.map_wlog = lw;
             p.lp.map_outer = static_cast<int64_t>(n_vox / static_cast<uint64_t>(o.grid_shape[2]));
-            const int64_t tiles = ((p.lp.map_outer + 31) / 32) * ((p.lp.map_fast + 3) / 4);
+            const int64_t per_outer = kLaneVoxelThreads >> lw;
+            const int64_t tiles = ((p.lp.map_outer + per_outer - 1) / per_outer) * ((p.lp.map_fast + wf - 1) / wf);
             p.lp.grid = dim3(static_cast<unsigned>(tiles), 1, 1);
         }
         // split mode stages three words per (transmit, voxel): base, fraction, phase cycles
@@ -634,6 +642,7 @@ int compound_impl(int32_t storage, const void* channel_data, const float* rx_coo
     a.frame_passes = plan.lp.passes;
     a.tx_chunk = plan.lp.tx_chunk;
     a.map_fast = plan.lp.map_fast;
+    a.map_wlog = plan.lp.map_wlog;
     a.map_outer = plan.lp.map_outer;
 
     const bool all_device = r_ch == kOnDevice && r_rx == kOnDevice && r_scan == kOnDevice && r_arr == kOnDevice &&
@@ -1353,6 +1362,7 @@ int batch_run(mach_b200_batch* b, const mach_b200_job* jobs, uint32_t n_jobs, cu
         bj.a.frame_passes = p.lp.passes;
         bj.a.tx_chunk = p.lp.tx_chunk;
         bj.a.map_fast = p.lp.map_fast;
+        bj.a.map_wlog = p.lp.map_wlog;
         bj.a.map_outer = p.lp.map_outer;
         bj.st = p.st;
         bj.st.status = dev->status;

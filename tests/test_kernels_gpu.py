@@ -121,3 +121,18 @@ def test_lane_voxel_sixteen_frames(cuda, storage, interp):
     warp = _run(w, kernel="warp")
     assert H.rel_l2(lane, warp) <= 2e-6
     assert H.nrms_db(lane, H.oracle(w, storage=storage)) <= -60.0
+
+
+@pytest.mark.parametrize("name,n_frames", [("compound", 1), ("volume3d", 16), ("volume3d", 3)])
+def test_lane_voxel_grid_tiles_are_bit_identical(cuda, name, n_frames):
+    """The voxel-to-warp assignment on a grid (4 x 8, 2 x 16, ... neighbours, edge tiles
+    partly empty) changes which thread sums a voxel, never the sum."""
+    if name == "compound":
+        w = H.small("compound", n_x=37, n_z=45, n_tx=3)  # extents not multiples of the tiles
+    else:
+        w = H.small("volume3d", n_side=7, n_elem_side=8, n_frames=n_frames, n_samples=1400)
+    base = _run(w, kernel="lane_voxel", grid_shape=False)
+    for tile_fast in (0, 2, 4, 8, 16):
+        got = _run(w, kernel="lane_voxel", tile_fast=tile_fast)
+        np.testing.assert_array_equal(got, base)
+    assert np.abs(base).max() > 0
