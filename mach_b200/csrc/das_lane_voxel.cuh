@@ -324,6 +324,66 @@ __device__ __forceinline__ void lane_voxel_tile(const DasArgs& a, int64_t tile, 
 
                 int row = (t0 * a.n_rx + e) * row_len;
                 const int tx_step = a.n_rx * row_len;
+                if constexpr (!SPLIT && NF == 1) {
+                    if (a.n_samples >= 3) {
+                        // Two transmits at a time with no branch between them, so that the
+                        // loads of both are in flight together.  A tap that is not taken reads
+                        // sample 1 of its row (inside every row) and is not accumulated.
+#pragma unroll 1
+                        for (int t = 0; t < nt; t += 2, row += 2 * tx_step) {
+                            float2 xv[2];
+                            float cwv[2], swv[2];
+                            bool okv[2];
+#pragma unroll
+                            for (int u = 0; u < 2; ++u) {
+                                const bool in = t + u < nt;
+                                const int si = (in ? t + u : t) * kLaneVoxelThreads + threadIdx.x;
+                                const float tau = __fmaf_rn(dist, a.inv_c, s_arrival[si]);
+                                const float sp = __fmul_rn(__fsub_rn(tau, a.t0), a.fs);
+                                bool ok = in && pair_ok && !(tau < 0.0f);
+                                if constexpr (INTERP == kNearest) {
+                                    ok = ok && (sp >= -0.5f) && (sp <= a.hi_nearest);
+                                } else if constexpr (INTERP == kLinear) {
+                                    ok = ok && (sp >= 0.0f) && (sp <= a.hi_linear);
+                                } else {
+                                    ok = ok && (sp >= 1.0f) && (sp <= a.hi_quadratic);
+                                }
+                                TapPosition tp = tap_position<INTERP>(sp);
+                                if constexpr (INTERP == kNearest) ok = ok && tp.idx < a.n_samples;
+                                if (!ok) {
+                                    tp.idx = 1;
+                                    tp.step = 0;
+                                }
+                                float cw = w, sw = 0.f;
+                                if (kCplx && a.rotate) {
+                                    float sn, cs;
+                                    __sincosf(__fmul_rn(a.mod_rad, tau), &sn, &cs);  // kernel.cu:656-658
+                                    cw = __fmul_rn(cs, w);
+                                    sw = __fmul_rn(sn, w);
+                                }
+                                const int row_u = in ? row + u * tx_step : row;
+                                xv[u] = tap_value<S, INTERP>(channel + (row_u + tp.idx * n_frames), tp, n_frames);
+                                cwv[u] = cw;
+                                swv[u] = sw;
+                                okv[u] = ok;
+                            }
+#pragma unroll
+                            for (int u = 0; u < 2; ++u) {
+                                const float2 x = xv[u];
+                                float2 r;
+                                if constexpr (kCplx) {
+                                    r.x = __fmaf_rn(x.x, cwv[u], __fmaf_rn(-x.y, swv[u], acc[0].x));
+                                    r.y = __fmaf_rn(x.y, cwv[u], __fmaf_rn(x.x, swv[u], acc[0].y));
+                                } else {
+                                    r.x = __fmaf_rn(x.x, cwv[u], acc[0].x);
+                                    r.y = acc[0].y;
+                                }
+                                acc[0] = okv[u] ? r : acc[0];
+                            }
+                        }
+                        continue;
+                    }
+                }
 #pragma unroll 2
                 for (int t = 0; t < nt; ++t, row += tx_step) {
                     const int si = t * kLaneVoxelThreads + threadIdx.x;
