@@ -324,7 +324,7 @@ __device__ __forceinline__ void lane_voxel_tile(const DasArgs& a, int64_t tile, 
 
                 int row = (t0 * a.n_rx + e) * row_len;
                 const int tx_step = a.n_rx * row_len;
-                if constexpr (!SPLIT && NF == 1) {
+                if constexpr (NF == 1) {
                     if (a.n_samples >= 3) {
                         // Two transmits at a time with no branch between them, so that the
                         // loads of both are in flight together.  A tap that is not taken reads
@@ -338,28 +338,49 @@ __device__ __forceinline__ void lane_voxel_tile(const DasArgs& a, int64_t tile, 
                             for (int u = 0; u < 2; ++u) {
                                 const bool in = t + u < nt;
                                 const int si = (in ? t + u : t) * kLaneVoxelThreads + threadIdx.x;
-                                const float tau = __fmaf_rn(dist, a.inv_c, s_arrival[si]);
-                                const float sp = __fmul_rn(__fsub_rn(tau, a.t0), a.fs);
-                                bool ok = in && pair_ok && !(tau < 0.0f);
-                                if constexpr (INTERP == kNearest) {
-                                    ok = ok && (sp >= -0.5f) && (sp <= a.hi_nearest);
-                                } else if constexpr (INTERP == kLinear) {
-                                    ok = ok && (sp >= 0.0f) && (sp <= a.hi_linear);
+                                TapPosition tp{};
+                                bool ok;
+                                float cw = w, sw = 0.f;
+                                if constexpr (SPLIT) {
+                                    int base = s_base[si] + rx_pos.base;
+                                    float frac = __fadd_rn(s_arrival[si], rx_pos.frac);
+                                    if (frac >= 1.0f) {
+                                        frac = __fsub_rn(frac, 1.0f);
+                                        base += 1;
+                                    }
+                                    ok = in && pair_ok &&
+                                         !(base < a.start_base || (base == a.start_base && frac < a.start_frac));
+                                    const bool inside = split_tap_position<INTERP>(base, frac, a.n_samples, tp);
+                                    ok = ok && inside;
+                                    if (kCplx && a.rotate) {
+                                        float sn, cs;
+                                        split_phasor(__fadd_rn(s_cyc[si], rx_cyc), sn, cs);
+                                        cw = __fmul_rn(cs, w);
+                                        sw = __fmul_rn(sn, w);
+                                    }
                                 } else {
-                                    ok = ok && (sp >= 1.0f) && (sp <= a.hi_quadratic);
+                                    const float tau = __fmaf_rn(dist, a.inv_c, s_arrival[si]);
+                                    const float sp = __fmul_rn(__fsub_rn(tau, a.t0), a.fs);
+                                    ok = in && pair_ok && !(tau < 0.0f);
+                                    if constexpr (INTERP == kNearest) {
+                                        ok = ok && (sp >= -0.5f) && (sp <= a.hi_nearest);
+                                    } else if constexpr (INTERP == kLinear) {
+                                        ok = ok && (sp >= 0.0f) && (sp <= a.hi_linear);
+                                    } else {
+                                        ok = ok && (sp >= 1.0f) && (sp <= a.hi_quadratic);
+                                    }
+                                    tp = tap_position<INTERP>(sp);
+                                    if constexpr (INTERP == kNearest) ok = ok && tp.idx < a.n_samples;
+                                    if (kCplx && a.rotate) {
+                                        float sn, cs;
+                                        __sincosf(__fmul_rn(a.mod_rad, tau), &sn, &cs);  // kernel.cu:656-658
+                                        cw = __fmul_rn(cs, w);
+                                        sw = __fmul_rn(sn, w);
+                                    }
                                 }
-                                TapPosition tp = tap_position<INTERP>(sp);
-                                if constexpr (INTERP == kNearest) ok = ok && tp.idx < a.n_samples;
                                 if (!ok) {
                                     tp.idx = 1;
                                     tp.step = 0;
-                                }
-                                float cw = w, sw = 0.f;
-                                if (kCplx && a.rotate) {
-                                    float sn, cs;
-                                    __sincosf(__fmul_rn(a.mod_rad, tau), &sn, &cs);  // kernel.cu:656-658
-                                    cw = __fmul_rn(cs, w);
-                                    sw = __fmul_rn(sn, w);
                                 }
                                 const int row_u = in ? row + u * tx_step : row;
                                 xv[u] = tap_value<S, INTERP>(channel + (row_u + tp.idx * n_frames), tp, n_frames);
