@@ -89,7 +89,9 @@ typedef struct mach_b200_options {
     int32_t kernel;          /* MACH_B200_KERNEL_*, 0 = automatic */
     int32_t tx_chunk;        /* lane-voxel kernel: transmits per shared-memory pass, 0 = automatic */
     int32_t window_rows;     /* staged / ensemble kernels: sample rows per window, 0 = automatic */
-    int32_t lanes_per_voxel; /* staged kernel: 4, 8, 16 or 32, 0 = automatic */
+    int32_t lanes_per_voxel; /* staged kernel: 4, 8, 16 or 32; one-frame voxel-per-lane kernel: 1, 2
+                                or 4 lanes per voxel, each summing every 2nd / 4th element;
+                                0 = automatic */
     int32_t tx_model;        /* MACH_B200_TX_ARRAYS: read tx_wave_arrivals_s; MACH_B200_TX_PLANE /
                                 MACH_B200_TX_SPHERICAL: every (point, transmit) arrival is formed on the
                                 device from tx_params, by one kernel into a temporary [n_tx][n_scan]

@@ -200,12 +200,13 @@ __device__ __forceinline__ float fast_tukey(float h2, float radius, const DasArg
 // warp takes wf = 2^map_wlog neighbours along the contiguous axis times 32 / wf along the next
 // one (a CTA wf x 128 / wf), so that the sample rows the 32 lanes of a load read lie close
 // together in memory (few L1 lines per warp load); otherwise a tile is 128 consecutive voxels.
+template <int VPC = kLaneVoxelThreads>
 __device__ __forceinline__ int64_t lane_voxel_index(const DasArgs& a, int64_t tile, int j) {
-    if (a.map_fast <= 0) return tile * kLaneVoxelThreads + j;
+    if (a.map_fast <= 0) return tile * VPC + j;
     const int lw = a.map_wlog;
     const int64_t tiles_fast = (a.map_fast + (1 << lw) - 1) >> lw;
     const int64_t to = tile / tiles_fast;
-    const int64_t o = to * (kLaneVoxelThreads >> lw) + (j >> lw);
+    const int64_t o = to * (VPC >> lw) + (j >> lw);
     const int64_t f = ((tile - to * tiles_fast) << lw) + (j & ((1 << lw) - 1));
     return (o < a.map_outer && f < a.map_fast) ? o * a.map_fast + f : a.n_vox;
 }
@@ -213,8 +214,12 @@ __device__ __forceinline__ int64_t lane_voxel_index(const DasArgs& a, int64_t ti
 // One CTA tile: voxels [tile * 128, tile * 128 + 128) of job `a`, all its transmits,
 // elements and frames.  `smem_words` is the dynamic shared memory (tx_chunk x 128 words,
 // x3 in split mode).  Shared by the per-job kernel and the persistent batch kernel.
-template <int S, int INTERP, int NF, bool SPLIT>
+// CS > 1 (one-frame jobs too small to fill the GPU): CS consecutive lanes share a voxel, each
+// summing every CS-th candidate element, and their sums are added with warp shuffles; a CTA
+// then covers 128 / CS voxels.
+template <int S, int INTERP, int NF, bool SPLIT, int CS = 1>
 __device__ __forceinline__ void lane_voxel_tile(const DasArgs& a, int64_t tile, float* smem_words) {
+    static_assert(CS == 1 || NF == 1, "channel split: one-frame jobs only");
     using ST = Storage<S>;
     using T = typename ST::T;
     constexpr bool kCplx = ST::kComplex;
@@ -225,7 +230,8 @@ __device__ __forceinline__ void lane_voxel_tile(const DasArgs& a, int64_t tile, 
     float* const s_cyc = s_arrival + 2 * a.tx_chunk * kLaneVoxelThreads;
 
     const int lane = threadIdx.x & 31;
-    const int64_t v = lane_voxel_index(a, tile, threadIdx.x);
+    const int sub = threadIdx.x & (CS - 1);  // this lane's share of the voxel's elements
+    const int64_t v = lane_voxel_index<kLaneVoxelThreads / CS>(a, tile, threadIdx.x / CS);
     const bool vox_ok = v < a.n_vox;
     const int n_frames = NF > 0 ? NF : a.n_frames;
 
@@ -294,8 +300,12 @@ __device__ __forceinline__ void lane_voxel_tile(const DasArgs& a, int64_t tile, 
                 }
             }
             unsigned cmask = __ballot_sync(kFull, cand);
-            while (cmask) {
-                const int e = eb + __ffs(cmask) - 1;
+            // CS > 1: lane `sub` of a voxel takes the candidates e with e % CS == sub, so a
+            // voxel's partial sums do not depend on which warp (tile) it is in.
+            if constexpr (CS > 1) cmask &= (CS == 4 ? 0x11111111u : 0x55555555u) << sub;
+            while (CS == 1 ? cmask != 0u : __any_sync(kFull, cmask != 0u)) {
+                const bool e_ok = cmask != 0u;
+                const int e = eb + (e_ok ? __ffs(cmask) - 1 : 0);
                 cmask &= cmask - 1u;
 
                 // Receive path (kernel.cu:444-483), reused for every transmit below.
@@ -318,7 +328,7 @@ __device__ __forceinline__ void lane_voxel_tile(const DasArgs& a, int64_t tile, 
                 }
                 float weight = 1.0f;
                 if (a.apod) weight = fast_tukey(h2, radius, a);
-                const bool pair_ok = vox_ok && !(h2 > radius_sq) && !(weight == 0.0f);
+                const bool pair_ok = vox_ok && e_ok && !(h2 > radius_sq) && !(weight == 0.0f);
                 if (!__any_sync(kFull, pair_ok)) continue;
                 const float w = __fmul_rn(weight, a.scale);
 
@@ -503,6 +513,17 @@ __device__ __forceinline__ void lane_voxel_tile(const DasArgs& a, int64_t tile, 
         }
     }
 
+    if constexpr (CS > 1) {  // add the lanes' partial sums of each voxel
+#pragma unroll
+        for (int off = 1; off < CS; off <<= 1) {
+#pragma unroll
+            for (int f = 0; f < kAcc; ++f) {
+                acc[f].x = __fadd_rn(acc[f].x, __shfl_xor_sync(kFull, acc[f].x, off));
+                acc[f].y = __fadd_rn(acc[f].y, __shfl_xor_sync(kFull, acc[f].y, off));
+            }
+        }
+        if (sub != 0) return;
+    }
     if (!vox_ok) return;
     if constexpr (kVec) {
 #pragma unroll
@@ -647,11 +668,11 @@ __device__ __forceinline__ float2 gather_taps(const typename Storage<S>::T* row,
     }
 }
 
-template <int S, int INTERP, int NF, bool SPLIT>
+template <int S, int INTERP, int NF, bool SPLIT, int CS = 1>
 __global__ void __launch_bounds__(kLaneVoxelThreads, NF == 16 ? 4 : 8)
     das_lane_voxel_kernel(const __grid_constant__ DasArgs a) {
     extern __shared__ float smem_words[];
-    lane_voxel_tile<S, INTERP, NF, SPLIT>(a, blockIdx.x, smem_words);
+    lane_voxel_tile<S, INTERP, NF, SPLIT, CS>(a, blockIdx.x, smem_words);
 }
 
 }  // namespace mach_b200

@@ -23,7 +23,7 @@ enum KernelKind : int {
 
 struct LaunchPlan {
     int kind;
-    int lanes_per_voxel;  // staged kernel: 4, 8, 16 or 32
+    int lanes_per_voxel;  // staged kernel: 4, 8, 16 or 32; one-frame lane-voxel kernel: 1, 2 or 4 lanes per voxel
     int passes;       // frames per lane (multi-frame kernels)
     int tx_chunk;     // arrivals staged per pass (lane-voxel kernels)
     dim3 grid;
@@ -86,10 +86,19 @@ cudaError_t launch_das(const DasArgs& a, int interp, const LaunchPlan& p, cudaSt
         if (a.split) das_lane_voxel_kernel<S, I, NF, true><<<p.grid, p.block, p.smem, stream>>>(a);  \
         else das_lane_voxel_kernel<S, I, NF, false><<<p.grid, p.block, p.smem, stream>>>(a);         \
     } while (0)
+#define MACH_B200_LV_CS(I, CS)                                                                           \
+    do {                                                                                                 \
+        if (a.split) das_lane_voxel_kernel<S, I, 1, true, CS><<<p.grid, p.block, p.smem, stream>>>(a);   \
+        else das_lane_voxel_kernel<S, I, 1, false, CS><<<p.grid, p.block, p.smem, stream>>>(a);          \
+    } while (0)
 #define MACH_B200_WG(I, L, P) das_gather_kernel<S, I, L, P><<<p.grid, p.block, 0, stream>>>(a)
 #define MACH_B200_KINDS(I)                                   \
     switch (p.kind) {                                        \
-        case kKindLaneVoxel1: MACH_B200_LV(I, 1); break;     \
+        case kKindLaneVoxel1:                                \
+            if (p.lanes_per_voxel == 4) MACH_B200_LV_CS(I, 4); \
+            else if (p.lanes_per_voxel == 2) MACH_B200_LV_CS(I, 2); \
+            else MACH_B200_LV(I, 1);                         \
+            break;                                           \
         case kKindLaneVoxelN: MACH_B200_LV(I, 0); break;     \
         case kKindLaneVoxel16: MACH_B200_LV(I, 16); break;   \
         case kKindWarpHalf: MACH_B200_WG(I, 16, 4); break;   \
@@ -102,6 +111,7 @@ cudaError_t launch_das(const DasArgs& a, int interp, const LaunchPlan& p, cudaSt
     }
 #undef MACH_B200_KINDS
 #undef MACH_B200_WG
+#undef MACH_B200_LV_CS
 #undef MACH_B200_LV
     return cudaGetLastError();
 }

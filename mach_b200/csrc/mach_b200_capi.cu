@@ -297,7 +297,19 @@ Plan plan_launch(int storage, uint64_t n_vox, uint32_t n_frames, uint32_t n_tx, 
         const uint32_t chunks = std::max<uint32_t>(1u, (n_tx + chunk - 1) / chunk);
         p.lp.tx_chunk = static_cast<int>(std::max<uint32_t>(1u, (n_tx + chunks - 1) / chunks));
         p.lp.block = dim3(kLaneVoxelThreads, 1, 1);
-        p.lp.grid = dim3(static_cast<unsigned>((n_vox + kLaneVoxelThreads - 1) / kLaneVoxelThreads), 1, 1);
+        // One-frame jobs that give fewer than 4 CTAs of 128 voxels per SM: 4 lanes per voxel,
+        // each summing a quarter of the elements (direct calls only; batches take 1).
+        int cs = 1;
+        if (n_frames <= 1 && interp >= 0) {
+            if (o.lanes_per_voxel == 1 || o.lanes_per_voxel == 2 || o.lanes_per_voxel == 4) {
+                cs = o.lanes_per_voxel;
+            } else if ((n_vox + kLaneVoxelThreads - 1) / kLaneVoxelThreads < 4u * 148u) {
+                cs = 4;
+            }
+        }
+        p.lp.lanes_per_voxel = cs;
+        const int vpc = kLaneVoxelThreads / cs;  // voxels per CTA
+        p.lp.grid = dim3(static_cast<unsigned>((n_vox + vpc - 1) / vpc), 1, 1);
         // On a known grid: CTA tiles of wf x (128 / wf) voxels, warps of wf x (32 / wf).
         // Automatic: 2 along the contiguous axis for 16 frames (rows of 32+ bytes), else 4.
         const int wf = o.tile_fast == 2 || o.tile_fast == 4 || o.tile_fast == 8 || o.tile_fast == 16
@@ -308,7 +320,7 @@ Plan plan_launch(int storage, uint64_t n_vox, uint32_t n_frames, uint32_t n_tx, 
             p.lp.map_fast = o.grid_shape[2];
             p.lp.map_wlog = lw;
             p.lp.map_outer = static_cast<int64_t>(n_vox / static_cast<uint64_t>(o.grid_shape[2]));
-            const int64_t per_outer = kLaneVoxelThreads >> lw;
+            const int64_t per_outer = vpc >> lw;
             const int64_t tiles = ((p.lp.map_outer + per_outer - 1) / per_outer) * ((p.lp.map_fast + wf - 1) / wf);
             p.lp.grid = dim3(static_cast<unsigned>(tiles), 1, 1);
         }

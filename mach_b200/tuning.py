@@ -38,7 +38,9 @@ def candidates(storage: str, n_frames: int, grid: Any) -> list[dict]:
     if n_frames <= 8 or n_frames == 16:
         for tx_chunk in (8, 16, 32):
             for tile_fast in ((2, 4, 8) if grid else (0,)):
-                out.append({"kernel": "lane_voxel", "tx_chunk": tx_chunk, "tile_fast": tile_fast})
+                for lanes in ((1, 4) if n_frames == 1 else (0,)):
+                    out.append({"kernel": "lane_voxel", "tx_chunk": tx_chunk, "tile_fast": tile_fast,
+                                "lanes_per_voxel": lanes})
     if n_frames % vf == 0 and n_frames > 1:
         lv_max = 32 if storage in ("f32", "c64") else 16
         needed = -(-n_frames // vf)
