@@ -297,14 +297,16 @@ Plan plan_launch(int storage, uint64_t n_vox, uint32_t n_frames, uint32_t n_tx, 
         const uint32_t chunks = std::max<uint32_t>(1u, (n_tx + chunk - 1) / chunk);
         p.lp.tx_chunk = static_cast<int>(std::max<uint32_t>(1u, (n_tx + chunks - 1) / chunks));
         p.lp.block = dim3(kLaneVoxelThreads, 1, 1);
-        // One-frame jobs that give fewer than 4 CTAs of 128 voxels per SM: 4 lanes per voxel,
-        // each summing a quarter of the elements (direct calls only; batches take 1).
+        // One-frame jobs split each voxel's elements over 2 or 4 lanes (direct calls only;
+        // batches take 1).  Measured on B200: 4 for jobs of fewer than 4 CTAs of 128 voxels
+        // per SM and for split delays, 2 otherwise.
         int cs = 1;
         if (n_frames <= 1 && interp >= 0) {
             if (o.lanes_per_voxel == 1 || o.lanes_per_voxel == 2 || o.lanes_per_voxel == 4) {
                 cs = o.lanes_per_voxel;
-            } else if ((n_vox + kLaneVoxelThreads - 1) / kLaneVoxelThreads < 4u * 148u) {
-                cs = 4;
+            } else {
+                const bool small = (n_vox + kLaneVoxelThreads - 1) / kLaneVoxelThreads < 4u * 148u;
+                cs = small || (o.flags & MACH_B200_FLAG_SPLIT_DELAY) ? 4 : 2;
             }
         }
         p.lp.lanes_per_voxel = cs;
