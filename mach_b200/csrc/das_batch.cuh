@@ -55,7 +55,7 @@ __device__ __forceinline__ void copy_words(T* dst, const T* src) {
     for (int i = threadIdx.x; i < static_cast<int>(sizeof(T) / 4); i += blockDim.x) d[i] = s[i];
 }
 
-template <int S, int INTERP, int NF, bool SPLIT>
+template <int S, int INTERP, int NF, bool SPLIT, int CS = 1>
 __global__ void __launch_bounds__(kLaneVoxelThreads, NF == 16 ? 4 : 8)
     das_lane_voxel_persistent(const BatchHeader* __restrict__ hdr, const BatchJob* __restrict__ jobs,
                               const int64_t* __restrict__ item_begin, unsigned long long* counter) {
@@ -67,7 +67,7 @@ __global__ void __launch_bounds__(kLaneVoxelThreads, NF == 16 ? 4 : 8)
     while (next_item(hdr, item_begin, counter, cursor, &s_job, &s_local)) {
         copy_words(&s_args, &jobs[s_job].a);
         __syncthreads();
-        lane_voxel_tile<S, INTERP, NF, SPLIT>(s_args, s_local, smem_words);
+        lane_voxel_tile<S, INTERP, NF, SPLIT, CS>(s_args, s_local, smem_words);
     }
 }
 

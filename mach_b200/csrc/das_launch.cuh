@@ -140,18 +140,21 @@ cudaError_t launch_persistent(K kernel, int threads, const PersistentLaunch& pl,
     return cudaGetLastError();
 }
 
-// Lane-voxel family: frame class 1 (one frame), 0 (2..8 frames), 16 (sixteen, vectorised).
+// Lane-voxel family: frame class 1 (one frame), 12 / 14 (one frame, 2 / 4 lanes per voxel),
+// 0 (2..8 frames), 16 (sixteen, vectorised).
 template <int S>
 cudaError_t launch_lane_voxel_persistent(int interp, int frame_class, bool split, const PersistentLaunch& pl,
                                          cudaStream_t stream) {
-#define MACH_B200_PLV(I, NF)                                                                              \
-    return split ? launch_persistent(das_lane_voxel_persistent<S, I, NF, true>, kLaneVoxelThreads, pl, stream) \
-                 : launch_persistent(das_lane_voxel_persistent<S, I, NF, false>, kLaneVoxelThreads, pl, stream)
+#define MACH_B200_PLV(I, NF, CS)                                                                              \
+    return split ? launch_persistent(das_lane_voxel_persistent<S, I, NF, true, CS>, kLaneVoxelThreads, pl, stream) \
+                 : launch_persistent(das_lane_voxel_persistent<S, I, NF, false, CS>, kLaneVoxelThreads, pl, stream)
 #define MACH_B200_PLV_NF(I)                         \
     switch (frame_class) {                          \
-        case 1: MACH_B200_PLV(I, 1);                \
-        case 16: MACH_B200_PLV(I, 16);              \
-        default: MACH_B200_PLV(I, 0);               \
+        case 1: MACH_B200_PLV(I, 1, 1);             \
+        case 12: MACH_B200_PLV(I, 1, 2);            \
+        case 14: MACH_B200_PLV(I, 1, 4);            \
+        case 16: MACH_B200_PLV(I, 16, 1);           \
+        default: MACH_B200_PLV(I, 0, 1);            \
     }
     switch (interp) {
         case kNearest: MACH_B200_PLV_NF(kNearest)

@@ -297,11 +297,10 @@ Plan plan_launch(int storage, uint64_t n_vox, uint32_t n_frames, uint32_t n_tx, 
         const uint32_t chunks = std::max<uint32_t>(1u, (n_tx + chunk - 1) / chunk);
         p.lp.tx_chunk = static_cast<int>(std::max<uint32_t>(1u, (n_tx + chunks - 1) / chunks));
         p.lp.block = dim3(kLaneVoxelThreads, 1, 1);
-        // One-frame jobs split each voxel's elements over 2 or 4 lanes (direct calls only;
-        // batches take 1).  Measured on B200: 4 for jobs of fewer than 4 CTAs of 128 voxels
-        // per SM and for split delays, 2 otherwise.
+        // One-frame jobs split each voxel's elements over 2 or 4 lanes.  Measured on B200: 4
+        // for jobs of fewer than 4 CTAs of 128 voxels per SM and for split delays, 2 otherwise.
         int cs = 1;
-        if (n_frames <= 1 && interp >= 0) {
+        if (n_frames <= 1) {
             if (o.lanes_per_voxel == 1 || o.lanes_per_voxel == 2 || o.lanes_per_voxel == 4) {
                 cs = o.lanes_per_voxel;
             } else {
@@ -1333,7 +1332,8 @@ int batch_run(mach_b200_batch* b, const mach_b200_job* jobs, uint32_t n_jobs, cu
         if (p.staged) {
             k = {1, j.storage, j.interp_type, p.lp.lanes_per_voxel, 0};
         } else if (p.lp.kind == kKindLaneVoxel1 || p.lp.kind == kKindLaneVoxelN || p.lp.kind == kKindLaneVoxel16) {
-            const int fc = p.lp.kind == kKindLaneVoxel1 ? 1 : (p.lp.kind == kKindLaneVoxel16 ? 16 : 0);
+            int fc = p.lp.kind == kKindLaneVoxel1 ? 1 : (p.lp.kind == kKindLaneVoxel16 ? 16 : 0);
+            if (fc == 1 && p.lp.lanes_per_voxel > 1) fc = 10 + p.lp.lanes_per_voxel;  // 12 / 14
             k = {0, j.storage, j.interp_type, fc, (j.flags & MACH_B200_FLAG_SPLIT_DELAY) ? 1 : 0};
         } else {
             return fail(MACH_B200_ERR_VALUE, "job %u: %u frames not a multiple of the storage's lane vector", i,

@@ -47,12 +47,6 @@ def _jobs_and_workloads():
     return out
 
 
-def _one_lane(w) -> dict:
-    """A single call sums a small one-frame job over 4 lanes per voxel (another summation
-    order); batches use one lane per voxel, which a single call also does when asked."""
-    return {"lanes_per_voxel": 1} if w.n_frames == 1 else {}
-
-
 def test_mixed_batch_matches_single_calls_and_oracle(cuda):
     import torch
 
@@ -65,7 +59,7 @@ def test_mixed_batch_matches_single_calls_and_oracle(cuda):
         torch.cuda.synchronize()
         for w, job in pairs:
             got = job.out.cpu().numpy()
-            alone = H.gpu_compound(w, **_one_lane(w))
+            alone = H.gpu_compound(w)
             assert np.array_equal(got, alone), (w.name, w.storage, H.rel_l2(got, alone))
             want = H.oracle(w)
             assert H.nrms_db(got, want) < -60, (w.name, w.storage)
@@ -106,7 +100,7 @@ def test_captured_batch_replays_with_new_channel_data(cuda):
         torch.cuda.synchronize()
         base = [j.out.clone() for _, j in pairs]
         for (w, j), b in zip(pairs, base):
-            assert np.array_equal(b.cpu().numpy(), H.gpu_compound(w, **_one_lane(w)))
+            assert np.array_equal(b.cpu().numpy(), H.gpu_compound(w))
         for _, j in pairs:
             j.channel.mul_(2)  # exact in binary floating point
         batch.replay()
