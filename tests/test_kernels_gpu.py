@@ -136,3 +136,26 @@ def test_lane_voxel_grid_tiles_are_bit_identical(cuda, name, n_frames):
         got = _run(w, kernel="lane_voxel", tile_fast=tile_fast)
         np.testing.assert_array_equal(got, base)
     assert np.abs(base).max() > 0
+
+
+@pytest.mark.parametrize("name,storage", [("compound", "c64"), ("compound", "cf16"), ("plain2d", "f32"),
+                                          ("volume3d", "i16")])
+def test_lane_voxel_lanes_per_voxel(cuda, name, storage):
+    """One-frame jobs summed by 1, 2 or 4 lanes per voxel (each lane every 2nd / 4th element,
+    partial sums added by warp shuffles) agree to FP32 rounding and with the oracle."""
+    import torch
+
+    if name == "compound":
+        w = H.small("compound", n_tx=5)
+    elif name == "plain2d":
+        w = H.small("plain2d")
+    else:
+        w = H.small("volume3d", n_side=10, n_elem_side=8, n_frames=1)
+    if storage == "cf16":
+        w.channel = torch.view_as_real(w.channel).to(torch.float16).contiguous()
+        w.storage = "cf16"
+    results = [_run(w, kernel="lane_voxel", lanes_per_voxel=lanes) for lanes in (1, 2, 4)]
+    assert np.abs(results[0]).max() > 0
+    for r in results[1:]:
+        assert H.rel_l2(r, results[0]) <= 1e-6
+    assert H.nrms_db(results[2], H.oracle(w, storage=storage)) <= -60.0
