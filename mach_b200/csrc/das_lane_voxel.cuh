@@ -233,7 +233,11 @@ __device__ __forceinline__ void lane_voxel_tile(const DasArgs& a, int64_t tile, 
     const int sub = threadIdx.x & (CS - 1);  // this lane's share of the voxel's elements
     const int64_t v = lane_voxel_index<kLaneVoxelThreads / CS>(a, tile, threadIdx.x / CS);
     const bool vox_ok = v < a.n_vox;
-    const int n_frames = NF > 0 ? NF : a.n_frames;
+    const int n_frames = NF > 0 ? NF : a.n_frames;  // frames this thread sums
+    // Frames per sample row, and this CTA's first frame: vector jobs with more frames than NF
+    // run blockIdx.y chunks of NF frames each.
+    const int fstride = a.n_frames;
+    const int f0 = NF >= 2 ? static_cast<int>(blockIdx.y) * NF : 0;
 
     float vx = 0.f, vy = 0.f, vz = 0.f;
     if (vox_ok) {
@@ -266,7 +270,7 @@ __device__ __forceinline__ void lane_voxel_tile(const DasArgs& a, int64_t tile, 
     for (int f = 0; f < kAcc; ++f) acc[f] = make_float2(0.f, 0.f);
 
     const T* const channel = static_cast<const T*>(a.channel);
-    const int row_len = a.n_samples * n_frames;  // samples per (transmit, element) row
+    const int row_len = a.n_samples * fstride;  // samples per (transmit, element) row
     const int tx_chunk = a.tx_chunk;
 
     for (int t0 = 0; t0 < a.n_tx; t0 += tx_chunk) {
@@ -461,18 +465,18 @@ __device__ __forceinline__ void lane_voxel_tile(const DasArgs& a, int64_t tile, 
                             sw = __fmul_rn(sn, w);
                         }
                     }
-                    const T* p = channel + (row + tp.idx * n_frames);
+                    const T* p = channel + (row + tp.idx * fstride + f0);
                     if constexpr (kVec) {
                         float2 va[kAcc], vb[kAcc], vc[kAcc];
                         if constexpr (INTERP == kNearest) {
                             load_frames<S, NF>(p, va);
                         } else if constexpr (INTERP == kLinear) {
                             load_frames<S, NF>(p, va);
-                            load_frames<S, NF>(p + tp.step * NF, vb);
+                            load_frames<S, NF>(p + tp.step * fstride, vb);
                         } else {
-                            load_frames<S, NF>(p - NF, va);
+                            load_frames<S, NF>(p - fstride, va);
                             load_frames<S, NF>(p, vb);
-                            load_frames<S, NF>(p + NF, vc);
+                            load_frames<S, NF>(p + fstride, vc);
                         }
 #pragma unroll
                         for (int q = 0; q < kAcc; ++q) {
@@ -529,7 +533,7 @@ __device__ __forceinline__ void lane_voxel_tile(const DasArgs& a, int64_t tile, 
 #pragma unroll
         for (int q = 0; q < kAcc; ++q) {
             if constexpr (kCplx) {
-                float2* out = static_cast<float2*>(a.out) + v * NF + q;
+                float2* out = static_cast<float2*>(a.out) + v * fstride + f0 + q;
                 float2 r = acc[q];
                 if (a.accumulate) {
                     const float2 prev = *out;
@@ -538,7 +542,7 @@ __device__ __forceinline__ void lane_voxel_tile(const DasArgs& a, int64_t tile, 
                 }
                 *out = r;
             } else {
-                float* out = static_cast<float*>(a.out) + v * NF + 2 * q;
+                float* out = static_cast<float*>(a.out) + v * fstride + f0 + 2 * q;
                 out[0] = a.accumulate ? __fadd_rn(out[0], acc[q].x) : acc[q].x;
                 out[1] = a.accumulate ? __fadd_rn(out[1], acc[q].y) : acc[q].y;
             }

@@ -19,6 +19,7 @@ enum KernelKind : int {
     kKindStaged = 4,       // das_staged_kernel, windows staged in shared memory (TMA or direct)
     kKindLaneVoxel16 = 5,  // das_lane_voxel_kernel, exactly 16 frames loaded as 16-byte vectors
     kKindEnsemble = 6,     // das_ensemble_kernel, windows in tensor memory, lanes = frames
+    kKindLaneVoxel8 = 7,   // das_lane_voxel_kernel, chunks of 8 frames (grid.y) of a longer ensemble
 };
 
 struct LaunchPlan {
@@ -101,6 +102,7 @@ cudaError_t launch_das(const DasArgs& a, int interp, const LaunchPlan& p, cudaSt
             break;                                           \
         case kKindLaneVoxelN: MACH_B200_LV(I, 0); break;     \
         case kKindLaneVoxel16: MACH_B200_LV(I, 16); break;   \
+        case kKindLaneVoxel8: MACH_B200_LV(I, 8); break;     \
         case kKindWarpHalf: MACH_B200_WG(I, 16, 4); break;   \
         default: MACH_B200_WG(I, 32, 8); break;              \
     }

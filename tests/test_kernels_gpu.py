@@ -159,3 +159,18 @@ def test_lane_voxel_lanes_per_voxel(cuda, name, storage):
     for r in results[1:]:
         assert H.rel_l2(r, results[0]) <= 1e-6
     assert H.nrms_db(results[2], H.oracle(w, storage=storage)) <= -60.0
+
+
+@pytest.mark.parametrize("storage", ["c64", "cf16", "cbf16", "ci16", "f16", "i16", "f32"])
+@pytest.mark.parametrize("n_frames", [24, 40])
+def test_lane_voxel_frame_chunks(cuda, storage, n_frames):
+    """Ensembles longer than 16 frames in chunks of 8 frames per CTA row (the automatic kernel
+    for 4-byte complex storage) give the ensemble / warp kernels' sums."""
+    w = _workload(storage, n_frames, 1)
+    chunks = _run(w, kernel="lane_voxel")
+    other = _run(w, kernel="warp")
+    assert np.abs(chunks).max() > 0
+    assert H.rel_l2(chunks, other) <= 2e-6
+    assert H.nrms_db(chunks, H.oracle(w, storage=storage)) <= -60.0
+    if storage in ("cf16", "cbf16", "ci16"):
+        np.testing.assert_array_equal(_run(w), chunks)  # the automatic choice
