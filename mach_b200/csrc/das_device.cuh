@@ -136,6 +136,7 @@ struct DasArgs {
     int32_t map_fast;
     int32_t map_wlog;
     int64_t map_outer;
+    int32_t frame_chunks;   // lane-voxel 8-frame chunks: CTA b takes tile b / frame_chunks, chunk b % frame_chunks
     int32_t start_base;     // floor(-t0 * fs): samples before it belong to tau < 0
     float start_frac;       // -t0 * fs - start_base
     double fs_d;            // sampling frequency

@@ -218,7 +218,7 @@ __device__ __forceinline__ int64_t lane_voxel_index(const DasArgs& a, int64_t ti
 // summing every CS-th candidate element, and their sums are added with warp shuffles; a CTA
 // then covers 128 / CS voxels.
 template <int S, int INTERP, int NF, bool SPLIT, int CS = 1>
-__device__ __forceinline__ void lane_voxel_tile(const DasArgs& a, int64_t tile, float* smem_words) {
+__device__ __forceinline__ void lane_voxel_tile(const DasArgs& a, int64_t tile, float* smem_words, int chunk = 0) {
     static_assert(CS == 1 || NF == 1, "channel split: one-frame jobs only");
     using ST = Storage<S>;
     using T = typename ST::T;
@@ -235,9 +235,9 @@ __device__ __forceinline__ void lane_voxel_tile(const DasArgs& a, int64_t tile, 
     const bool vox_ok = v < a.n_vox;
     const int n_frames = NF > 0 ? NF : a.n_frames;  // frames this thread sums
     // Frames per sample row, and this CTA's first frame: vector jobs with more frames than NF
-    // run blockIdx.y chunks of NF frames each.
+    // run in chunks of NF frames.
     const int fstride = a.n_frames;
-    const int f0 = NF >= 2 ? static_cast<int>(blockIdx.y) * NF : 0;
+    const int f0 = NF >= 2 ? chunk * NF : 0;
 
     float vx = 0.f, vy = 0.f, vz = 0.f;
     if (vox_ok) {
@@ -676,7 +676,13 @@ template <int S, int INTERP, int NF, bool SPLIT, int CS = 1>
 __global__ void __launch_bounds__(kLaneVoxelThreads, NF == 16 ? 4 : 8)
     das_lane_voxel_kernel(const __grid_constant__ DasArgs a) {
     extern __shared__ float smem_words[];
-    lane_voxel_tile<S, INTERP, NF, SPLIT, CS>(a, blockIdx.x, smem_words);
+    if (NF >= 2 && a.frame_chunks > 1) {  // consecutive CTAs: the chunks of one tile, which share rows
+        const int64_t tile = blockIdx.x / a.frame_chunks;
+        lane_voxel_tile<S, INTERP, NF, SPLIT, CS>(a, tile, smem_words,
+                                                  static_cast<int>(blockIdx.x - tile * a.frame_chunks));
+    } else {
+        lane_voxel_tile<S, INTERP, NF, SPLIT, CS>(a, blockIdx.x, smem_words);
+    }
 }
 
 }  // namespace mach_b200

@@ -33,6 +33,7 @@ struct LaunchPlan {
     int map_fast;       // lane-voxel kernels: grid tiling (DasArgs::map_*), 0 = linear tiles
     int map_wlog;
     int64_t map_outer;
+    int frame_chunks;   // lane-voxel 8-frame chunks per tile (DasArgs::frame_chunks)
 };
 
 // Opt a kernel into more than 48 KB of dynamic shared memory (once per instance is enough,

@@ -338,7 +338,10 @@ Plan plan_launch(int storage, uint64_t n_vox, uint32_t n_frames, uint32_t n_tx, 
             const int64_t tiles = ((p.lp.map_outer + per_outer - 1) / per_outer) * ((p.lp.map_fast + wf - 1) / wf);
             p.lp.grid = dim3(static_cast<unsigned>(tiles), 1, 1);
         }
-        if (p.lp.kind == kKindLaneVoxel8) p.lp.grid.y = n_frames / 8;  // one CTA row per 8-frame chunk
+        if (p.lp.kind == kKindLaneVoxel8) {  // the 8-frame chunks of a tile run on consecutive CTAs
+            p.lp.frame_chunks = static_cast<int>(n_frames / 8);
+            p.lp.grid.x *= static_cast<unsigned>(p.lp.frame_chunks);
+        }
         // split mode stages three words per (transmit, voxel): base, fraction, phase cycles
         p.lp.smem = static_cast<size_t>(p.lp.tx_chunk) * kLaneVoxelThreads * sizeof(float) *
                     ((o.flags & MACH_B200_FLAG_SPLIT_DELAY) ? 3 : 1);
@@ -671,6 +674,7 @@ int compound_impl(int32_t storage, const void* channel_data, const float* rx_coo
     a.map_fast = plan.lp.map_fast;
     a.map_wlog = plan.lp.map_wlog;
     a.map_outer = plan.lp.map_outer;
+    a.frame_chunks = plan.lp.frame_chunks;
 
     const bool all_device = r_ch == kOnDevice && r_rx == kOnDevice && r_scan == kOnDevice && r_arr == kOnDevice &&
                             r_out == kOnDevice;
