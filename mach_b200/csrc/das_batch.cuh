@@ -67,7 +67,13 @@ __global__ void __launch_bounds__(kLaneVoxelThreads, NF == 16 ? 4 : 8)
     while (next_item(hdr, item_begin, counter, cursor, &s_job, &s_local)) {
         copy_words(&s_args, &jobs[s_job].a);
         __syncthreads();
-        lane_voxel_tile<S, INTERP, NF, SPLIT, CS>(s_args, s_local, smem_words);
+        if (NF >= 2 && s_args.frame_chunks > 1) {  // items: the 8-frame chunks of each tile
+            const int64_t tile = s_local / s_args.frame_chunks;
+            lane_voxel_tile<S, INTERP, NF, SPLIT, CS>(s_args, tile, smem_words,
+                                                      static_cast<int>(s_local - tile * s_args.frame_chunks));
+        } else {
+            lane_voxel_tile<S, INTERP, NF, SPLIT, CS>(s_args, s_local, smem_words);
+        }
     }
 }
 

@@ -144,7 +144,7 @@ cudaError_t launch_persistent(K kernel, int threads, const PersistentLaunch& pl,
 }
 
 // Lane-voxel family: frame class 1 (one frame), 12 / 14 (one frame, 2 / 4 lanes per voxel),
-// 0 (2..8 frames), 16 (sixteen, vectorised).
+// 0 (2..8 frames), 16 (sixteen, vectorised), 8 (chunks of 8 frames of a longer ensemble).
 template <int S>
 cudaError_t launch_lane_voxel_persistent(int interp, int frame_class, bool split, const PersistentLaunch& pl,
                                          cudaStream_t stream) {
@@ -157,6 +157,7 @@ cudaError_t launch_lane_voxel_persistent(int interp, int frame_class, bool split
         case 12: MACH_B200_PLV(I, 1, 2);            \
         case 14: MACH_B200_PLV(I, 1, 4);            \
         case 16: MACH_B200_PLV(I, 16, 1);           \
+        case 8: MACH_B200_PLV(I, 8, 1);             \
         default: MACH_B200_PLV(I, 0, 1);            \
     }
     switch (interp) {

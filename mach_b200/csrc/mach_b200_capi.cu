@@ -266,10 +266,10 @@ Plan plan_launch(int storage, uint64_t n_vox, uint32_t n_frames, uint32_t n_tx, 
     const int esz = static_cast<int>(storage_bytes(storage));
     const int vf = 8 / esz;
     int kind = o.kernel;
-    // Longer ensembles in chunks of 8 frames (one CTA row per chunk) of the voxel-per-lane
+    // Longer ensembles in chunks of 8 frames (one CTA per chunk and tile) of the voxel-per-lane
     // kernel: rows of 8 frames must be 16-byte vectors and every sample row a multiple of 16
-    // bytes.  Direct calls only (the batch kernels take one CTA row).
-    const bool lane8_ok = interp >= 0 && n_frames > 16 && n_frames % 8 == 0 && (8u * esz) % 16u == 0 &&
+    // bytes.
+    const bool lane8_ok = n_frames > 16 && n_frames % 8 == 0 && (8u * esz) % 16u == 0 &&
                           (static_cast<uint64_t>(n_frames) * esz) % 16u == 0 &&
                           (!channel_on_device || reinterpret_cast<uintptr_t>(channel) % 16 == 0);
     // Measured on B200 (200-frame Doppler): for 4-byte complex storage (cf16, cbf16, ci16) the
@@ -1349,8 +1349,10 @@ int batch_run(mach_b200_batch* b, const mach_b200_job* jobs, uint32_t n_jobs, cu
         GroupKey k{};
         if (p.staged) {
             k = {1, j.storage, j.interp_type, p.lp.lanes_per_voxel, 0};
-        } else if (p.lp.kind == kKindLaneVoxel1 || p.lp.kind == kKindLaneVoxelN || p.lp.kind == kKindLaneVoxel16) {
-            int fc = p.lp.kind == kKindLaneVoxel1 ? 1 : (p.lp.kind == kKindLaneVoxel16 ? 16 : 0);
+        } else if (p.lp.kind == kKindLaneVoxel1 || p.lp.kind == kKindLaneVoxelN || p.lp.kind == kKindLaneVoxel16 ||
+                   p.lp.kind == kKindLaneVoxel8) {
+            int fc = p.lp.kind == kKindLaneVoxel1 ? 1
+                     : (p.lp.kind == kKindLaneVoxel16 ? 16 : (p.lp.kind == kKindLaneVoxel8 ? 8 : 0));
             if (fc == 1 && p.lp.lanes_per_voxel > 1) fc = 10 + p.lp.lanes_per_voxel;  // 12 / 14
             k = {0, j.storage, j.interp_type, fc, (j.flags & MACH_B200_FLAG_SPLIT_DELAY) ? 1 : 0};
         } else {
@@ -1396,6 +1398,7 @@ int batch_run(mach_b200_batch* b, const mach_b200_job* jobs, uint32_t n_jobs, cu
         bj.a.map_fast = p.lp.map_fast;
         bj.a.map_wlog = p.lp.map_wlog;
         bj.a.map_outer = p.lp.map_outer;
+        bj.a.frame_chunks = p.lp.frame_chunks;
         bj.st = p.st;
         bj.st.status = dev->status;
         bj.tiles = static_cast<int32_t>(p.lp.grid.x);
