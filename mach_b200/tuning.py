@@ -35,6 +35,9 @@ def candidates(storage: str, n_frames: int, grid: Any) -> list[dict]:
     vf = 8 // esz
     out: list[dict] = []
     grids = [None, False] if grid else [False]
+    if n_frames > 16 and n_frames % 8 == 0:  # the voxel-per-lane kernel in 8-frame chunks
+        for tile_fast in ((2, 4) if grid else (0,)):
+            out.append({"kernel": "lane_voxel", "tile_fast": tile_fast})
     if n_frames <= 8 or n_frames == 16:
         for tx_chunk in (8, 16, 32):
             for tile_fast in ((2, 4, 8) if grid else (0,)):

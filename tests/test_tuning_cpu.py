@@ -9,6 +9,17 @@ def test_candidates_cover_the_families():
     kinds = {c["kernel"] for c in tuning.candidates("cf16", 16, None)}
     assert kinds == {"lane_voxel", "staged", "warp"}
     assert {c["kernel"] for c in tuning.candidates("f32", 1, None)} == {"lane_voxel"}
+    # long ensembles: 8-frame chunks of the voxel-per-lane kernel next to the ensemble kernel
+    kinds = {c["kernel"] for c in tuning.candidates("cf16", 200, (1, 256, 256))}
+    assert {"lane_voxel", "ensemble", "staged", "warp"} <= kinds
+
+
+def test_lane_voxel_knobs():
+    one = [c for c in tuning.candidates("c64", 1, (1, 512, 512)) if c["kernel"] == "lane_voxel"]
+    assert {c["lanes_per_voxel"] for c in one} == {1, 4}
+    assert {c["tile_fast"] for c in one} == {2, 4, 8}
+    no_grid = [c for c in tuning.candidates("c64", 1, None) if c["kernel"] == "lane_voxel"]
+    assert {c["tile_fast"] for c in no_grid} == {0}
 
 
 def test_staged_lanes_respect_storage_limits():
