@@ -5,7 +5,7 @@ from mach_b200 import tuning
 
 def test_candidates_cover_the_families():
     kinds = {c["kernel"] for c in tuning.candidates("c64", 64, (1, 256, 256))}
-    assert kinds == {"staged", "ensemble", "warp"}
+    assert kinds == {"staged", "ensemble", "warp", "lane_voxel"}
     kinds = {c["kernel"] for c in tuning.candidates("cf16", 16, None)}
     assert kinds == {"lane_voxel", "staged", "warp"}
     assert {c["kernel"] for c in tuning.candidates("f32", 1, None)} == {"lane_voxel"}
