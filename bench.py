@@ -1,20 +1,25 @@
 #!/usr/bin/env python
 """Benchmark: delay-and-sum throughput in points/s (voxel x channel x transmit x frame).
 
-One step = one complete beamforming job of the chosen workload (default: 75-transmit
-coherent compounding, 128 elements, 512x512 grid, 3328 complex64 IQ samples, quadratic
-interpolation, f# 1.75) with every input already in HBM.  Prints ONE JSON line on rank 0.
+One step = one complete beamforming job of the chosen workload with every input already in
+HBM.  The default workload is the largest single-GPU configuration: 3-D DAS, 9 diverging
+waves, 32 x 32 matrix array (1024 elements), 128^3 voxels, 2048 int16 RF samples x 16
+frames, linear interpolation, f# 1.0.  The same JSON line also carries, under "workloads",
+the Doppler ensemble (5 plane waves x 200 frames, 256^2, complex64 and FP16 IQ storage)
+measured the same way in the same process.  Prints ONE JSON line on rank 0.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                   [--workload compound|doppler|plain2d|volume3d|volume3d16|serving|rf2iq|ingest]
-                  [--storage c64|cf16|...]
+                  [--storage c64|cf16|...] [--also doppler:c64,doppler:cf16 | --also none]
 
 rf2iq and ingest time the front end before the beamformer (RF -> IQ by the analytic signal,
 and the acquisition-order rearrange) in channel samples/s.
 
 --impl reference times mach's own CUDA kernel (built from its unmodified source into
 oracle/_ref) on the same inputs, driven as mach drives it: one launch and one
-cudaDeviceSynchronize per transmit into a zeroed output.
+cudaDeviceSynchronize per transmit into a zeroed output, float32 / complex64 input (int16
+and FP16 storage are widened for it, as mach only takes those two types).  That process
+imports nothing of mach_b200 that opens its CUDA library.
 
 Multi-GPU (torchrun): every rank runs its own full job on its own GPU (voxels and jobs are
 independent; there is no data exchange), so scaling is weak; the time is the max over ranks.
@@ -70,13 +75,19 @@ def parse_args():
     p.add_argument("--steps", type=int, default=20)
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    p.add_argument("--workload", choices=sorted(WORKLOAD_DESC), default="compound")
+    p.add_argument("--workload", choices=sorted(WORKLOAD_DESC), default="volume3d16")
     p.add_argument("--storage", default=None, help="channel storage (default: the workload's own)")
     p.add_argument("--cpu-seconds", type=float, default=10.0, help="target CPU time of the cpu_baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--frames", type=int, default=None, help="override the workload's frame count (profiling)")
     p.add_argument("--side", type=int, default=None, help="override the 3-D grid side (profiling)")
+    p.add_argument("--also", default=None,
+                   help="extra workload:storage lines measured in the same run (default with the default "
+                        "workload: doppler:c64,doppler:cf16; 'none' for none)")
+    p.add_argument("--tune", action="store_true", help="run the autotuner on the job during warm-up")
+    p.add_argument("--launch", default="",
+                   help="launch options for the headline job, e.g. kernel=frame_lane,frame_slots=4 (profiling)")
     return p.parse_args()
 
 
@@ -178,14 +189,71 @@ def measured_peak_hbm():
     return 6650.0, "fallback"
 
 
-def profiled_traffic(key: str):
-    path = REPO / "profiles" / "dram_traffic.json"
+def profiled_traffic(key: str) -> dict:
+    """DRAM and L2 bytes per launch of the dominant kernel of a workload, from one ncu capture
+    summarised in profiles/ncu_traffic.json (not measured in this run)."""
+    path = REPO / "profiles" / "ncu_traffic.json"
     if path.exists():
-        table = json.loads(path.read_text())
-        entry = table.get(key)
+        entry = json.loads(path.read_text()).get(key)
         if entry:
-            return entry.get("bytes_per_launch")
-    return None
+            return entry
+    return {}
+
+
+_L2_PEAK = None
+
+
+def l2_peak_gbs() -> float | None:
+    """L2 read bandwidth of this GPU, measured now with the library's probe kernel: 16-byte
+    L1-bypassing loads over a 32 MB and a 64 MB buffer (both well inside the 126 MB L2), the
+    best of 5 timed launches of 8 passes each after one untimed launch; the larger of the two."""
+    global _L2_PEAK
+    if _L2_PEAK is not None:
+        return _L2_PEAK
+    from mach_b200 import _cuda_impl
+
+    best = 0.0
+    stream = torch.cuda.current_stream()
+    for mb in (32, 64):
+        buf = torch.ones(mb << 18, dtype=torch.float32, device="cuda")
+        nbytes = buf.numel() * 4
+        _cuda_impl.probe_l2_read(buf.data_ptr(), nbytes, 1, stream.cuda_stream)
+        for _ in range(5):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            _cuda_impl.probe_l2_read(buf.data_ptr(), nbytes, 8, stream.cuda_stream)
+            b.record(stream)
+            b.synchronize()
+            best = max(best, nbytes * 8 / (a.elapsed_time(b) * 1e-3) / 1e9)
+        del buf
+    _L2_PEAK = best
+    return best
+
+
+def roofline(w, storage, kernel_s, key) -> dict:
+    """HBM roofline of the dominant kernel (algorithmic bytes / CUDA-event time) with the DRAM
+    and L2 bytes of its ncu capture beside it (L2 against the probed L2 read bandwidth)."""
+    peak, peak_kind = measured_peak_hbm()
+    alg = algorithmic_bytes(w, storage)
+    achieved = alg / kernel_s / 1e9
+    prof = profiled_traffic(key)
+    r = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+         "traffic": prof.get("dram_bytes"), "algorithmic_bytes_per_launch": alg, "kernel_ms": kernel_s * 1e3,
+         "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs, copy bandwidth)" if peak_kind == "measured"
+         else "fallback 6650 GB/s"}
+    if prof:
+        r["traffic_source"] = f"ncu capture, not this run: {prof.get('source', '')}"
+    l2_peak = l2_peak_gbs()
+    lts = prof.get("lts_bytes")
+    if lts:
+        r["l2_bytes_per_launch"] = lts
+        r["l2_achieved"] = lts / kernel_s / 1e9
+    if l2_peak:
+        r["l2_peak"] = l2_peak
+        r["l2_peak_source"] = "mach_b200_probe_l2_read in this run (ld.global.cg over 32/64 MB)"
+        if lts:
+            r["l2_frac"] = r["l2_achieved"] / l2_peak
+    return r
 
 
 # ----------------------------------------------------------------------------- workloads
@@ -227,11 +295,55 @@ def algorithmic_bytes(w, storage) -> int:
 # ----------------------------------------------------------------------------- our arm
 
 
-def run_ours(args, world, rank, local):
-    from mach_b200 import _cuda_impl, _dlpack, experimental
+def workload_config(name, w, storage, world) -> dict:
+    """The `config` of a line: identical in both arms for the same workload."""
+    return {
+        "workload": f"{name}: {WORKLOAD_DESC[name]}",
+        "storage": storage,
+        "n_tx": w.n_tx, "n_rx": w.n_rx, "n_samples": w.n_samples, "n_frames": w.n_frames, "n_vox": w.n_vox,
+        "points_per_step": w.points,
+        "l2": f"inputs larger than L2 ({algorithmic_bytes(w, storage) / 1e6:.0f} MB per step > 126 MB), no flush",
+        "parallelism": f"replicas x{world} (one job per GPU, no exchange)",
+    }
 
-    w = make_workload(args.workload, args.frames, args.side)
-    storage = args.storage or w.storage
+
+def delay_mode(storage: str) -> str:
+    return "split" if storage in ("f16", "cf16", "bf16", "cbf16") else "reference"
+
+
+def parse_also(args) -> list[tuple[str, str | None]]:
+    spec = args.also
+    if spec is None:
+        spec = "doppler:c64,doppler:cf16" if args.workload == "volume3d16" and not args.frames and not args.side \
+            else "none"
+    if spec.strip().lower() in ("", "none"):
+        return []
+    out = []
+    for item in spec.split(","):
+        name, _, storage = item.strip().partition(":")
+        if name not in WORKLOAD_DESC or name in ("serving", "rf2iq", "ingest"):
+            raise SystemExit(f"--also: unknown beamforming workload {name!r}")
+        out.append((name, storage or None))
+    return out
+
+
+def run_ours(args, world, rank, local):
+    line = measure_ours(args, args.workload, args.storage, world, rank, local, headline=True)
+    also = parse_also(args)
+    if also:
+        line["workloads"] = [measure_ours(args, name, storage, world, rank, local, headline=False)
+                             for name, storage in also]
+    return line
+
+
+def measure_ours(args, name, storage, world, rank, local, headline):
+    """One workload through the C ABI (kernel-only `value`, device-resident inputs), its e2e
+    through the public API, and on rank 0 its accuracy (and, for the headline, the CPU baseline)."""
+    from mach_b200 import _cuda_impl, _dlpack, _grid
+
+    frames, side = (args.frames, args.side) if headline else (None, None)
+    w = make_workload(name, frames, side)
+    storage = storage or w.storage
     ch = storage_channel(w, storage)
     dev = torch.device("cuda", local)
     rx = torch.as_tensor(w.rx_coords_m, device=dev)
@@ -246,15 +358,31 @@ def run_ours(args, world, rank, local):
                   f_number=p["f_number"], rx_start_s=p["rx_start_s"], sampling_freq_hz=p["sampling_freq_hz"],
                   sound_speed_m_s=p["sound_speed_m_s"], modulation_freq_hz=p["modulation_freq_hz"],
                   tukey_alpha=p["tukey_alpha"], interp_type=p["interp_type"], channel_scale=w.storage_scale)
+    grid_shape = _grid.detect(w.scan_coords_m)
+    knobs = {}
+    if headline and args.launch:
+        for item in args.launch.split(","):
+            key, _, val = item.partition("=")
+            knobs[key.strip()] = val.strip() if key.strip() == "kernel" else int(val)
+    if args.tune:
+        from mach_b200 import tuning
 
-    from mach_b200 import _grid
-
-    options = _cuda_impl.make_options(grid_shape=_grid.detect(w.scan_coords_m))
+        knobs = tuning.tune(ch, rx, scan, arr, channel_scale=w.storage_scale, delay=delay_mode(storage), **p)
+        grid_shape = knobs.pop("grid_shape", grid_shape)
+        if grid_shape is False:
+            grid_shape = None
+    options = _cuda_impl.make_options(grid_shape=grid_shape, **knobs)
+    flags = _cuda_impl.FLAG_ASYNC | _cuda_impl.FLAG_OVERWRITE
+    # Storage whose samples are exact in FP32 (float32, complex64, int16 x scale) uses mach's
+    # FP32 delay arithmetic (bit-identical sample positions); FP16 / BF16 storage uses split
+    # delays, the API's default for it.
+    delay = delay_mode(storage)
+    if delay == "split":
+        flags |= _cuda_impl.FLAG_SPLIT_DELAY
 
     def step():
         _cuda_impl.beamform_compound(v_ch, storage, v_rx, v_scan, v_arr, v_out, stream=stream.cuda_stream,
-                                     flags=_cuda_impl.FLAG_ASYNC | _cuda_impl.FLAG_OVERWRITE, options=options,
-                                     **common)
+                                     flags=flags, options=options, **common)
 
     clocks = ClockSampler(local)
     clocks.start()
@@ -293,37 +421,30 @@ def run_ours(args, world, rank, local):
         "vs_baseline": None,
         "dtype": "f32",
         "data": "synthetic (seeded simulation of the configuration; no public dataset offline)",
-        "config": {
-            "workload": f"{args.workload}: {WORKLOAD_DESC[args.workload]}",
-            "storage": storage,
-            "n_tx": w.n_tx, "n_rx": w.n_rx, "n_samples": w.n_samples, "n_frames": w.n_frames, "n_vox": w.n_vox,
-            "points_per_step": w.points,
-            "l2": f"inputs larger than L2 ({algorithmic_bytes(w, storage) / 1e6:.0f} MB per step > 126 MB), no flush",
-            "parallelism": f"replicas x{world} (one job per GPU, no exchange)",
-        },
+        "config": workload_config(name, w, storage, world),
         "latency_ms": {"p50": float(np.percentile(per_step, 50)), "p99": float(np.percentile(per_step, 99))},
         "gpu_launches": int(launches),
+        "launch": {"delay": delay,
+                   "grid_shape": list(grid_shape) if grid_shape else None, "knobs": knobs or None,
+                   "tuned": bool(args.tune)},
     }
     kernel_s = statistics.mean(per_step) / 1e3
-    peak, peak_kind = measured_peak_hbm()
-    alg = algorithmic_bytes(w, storage)
-    achieved = alg / kernel_s / 1e9
-    line["roofline"] = {
-        "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-        "traffic": profiled_traffic(f"{args.workload}:{storage}"),
-        "algorithmic_bytes_per_launch": alg, "kernel_ms": kernel_s * 1e3, "peak_source": peak_kind,
-    }
+    line["roofline"] = roofline(w, storage, kernel_s, f"{name}:{storage}")
     line["clocks"] = clock_info
-
     if not args.no_e2e:
-        line["e2e"] = run_e2e(args, w, storage, ch, world, local)
+        line["e2e"] = run_e2e(args, w, storage, ch, world, local, knobs)
     if rank == 0 and world == 1:
-        line.update(accuracy_and_baselines(args, w, storage, result))
+        line.update(accuracy_and_baselines(args, w, storage, result, cpu_baseline=headline))
+    del ch, rx, scan, arr, out, result, v_ch, v_out
+    w.channel = None
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
     return line
 
 
-def accuracy_and_baselines(args, w, storage, result):
-    """nRMS against the FP64 oracle on a voxel sample (which also gives the CPU baseline rate)."""
+def accuracy_and_baselines(args, w, storage, result, cpu_baseline=True):
+    """nRMS against the FP64 oracle on a voxel sample (which also gives the CPU baseline rate),
+    and relative L2 against mach's kernel on the whole job."""
     from oracle import das_fp64, machref, oracle_c
 
     extra = {}
@@ -343,7 +464,7 @@ def accuracy_and_baselines(args, w, storage, result):
 
     n_sub = 256
     sel, y, dt = oracle_on(n_sub, ch_np, storage, w.storage_scale)
-    if not args.no_cpu_baseline:
+    if cpu_baseline and not args.no_cpu_baseline:
         while dt < 0.25 * args.cpu_seconds and n_sub < w.n_vox:
             n_sub = int(min(w.n_vox, n_sub * max(2.0, 0.5 * args.cpu_seconds / max(dt, 1e-3))))
             sel, y, dt = oracle_on(n_sub, ch_np, storage, w.storage_scale)
@@ -368,7 +489,10 @@ def accuracy_and_baselines(args, w, storage, result):
         acc["nrms_db_vs_fp64_oracle_on_source_data"] = das_fp64.nrms_db(got, y_src)
     if machref.available() and w.storage in ("c64", "f32", "i16"):
         ref = reference_once(w)
-        acc["rel_l2_vs_reference_kernel"] = das_fp64.rel_l2(result.cpu().numpy(), ref)
+        # mach takes float32 / complex64 only: int16 is widened exactly, so the same samples;
+        # FP16 / BF16 storage is compared against mach on the unrounded source data.
+        key = "rel_l2_vs_reference_kernel" if storage == w.storage else "rel_l2_vs_reference_kernel_on_source_data"
+        acc[key] = das_fp64.rel_l2(result.cpu().numpy(), ref)
     extra["accuracy"] = acc
     return extra
 
@@ -404,7 +528,7 @@ def reference_once(w):
     return out.cpu().numpy()
 
 
-def run_e2e(args, w, storage, ch_dev, world, local):
+def run_e2e(args, w, storage, ch_dev, world, local, knobs=None):
     """Same job through the public API with pinned host buffers: H2D + kernel + D2H per step."""
     from mach_b200 import experimental
 
@@ -418,7 +542,8 @@ def run_e2e(args, w, storage, ch_dev, world, local):
     def step():
         with warnings.catch_warnings():
             warnings.simplefilter("ignore", UserWarning)
-            experimental.beamform(ch_h, rx_h, scan_h, arr_h, out=out_h, channel_scale=w.storage_scale, **w.params)
+            experimental.beamform(ch_h, rx_h, scan_h, arr_h, out=out_h, channel_scale=w.storage_scale, **w.params,
+                                  delay=delay_mode(storage), **(knobs or {}))
 
     for _ in range(max(1, min(args.warmup, 3))):
         step()
@@ -705,7 +830,10 @@ def run_frontend(args, world, rank, local):
         "latency_ms": {"p50": float(np.percentile(per_step, 50)), "p99": float(np.percentile(per_step, 99))},
         "gpu_launches": int(launches),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": profiled_traffic(f"{args.workload}:{storage}"), "algorithmic_bytes_per_launch": alg,
+                     "traffic": profiled_traffic(f"{args.workload}:{storage}").get("dram_bytes"),
+                     "traffic_source": "ncu capture, not this run: "
+                                       + profiled_traffic(f"{args.workload}:{storage}").get("source", ""),
+                     "algorithmic_bytes_per_launch": alg,
                      "kernel_ms": kernel_s * 1e3, "peak_source": peak_kind},
         "clocks": clock_info,
     }
@@ -798,11 +926,26 @@ def run_frontend_reference(args, world, rank, local):
 def run_reference(args, world, rank, local):
     from oracle import machref
 
-    base = {"metric": METRIC, "unit": "points/s", "impl": "reference", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "higher_is_better": True}
     if not machref.available():
         return {"impl": "reference", "unavailable": "mach's kernel was not built into oracle/_ref (no reference checkout)"}
-    w = make_workload(args.workload, args.frames, args.side)
+    line = measure_reference(args, args.workload, args.storage, world, headline=True)
+    names = []
+    for name, _ in parse_also(args):
+        if name not in names:
+            names.append(name)
+    if names:
+        line["workloads"] = [measure_reference(args, name, None, world, headline=False) for name in names]
+    return line
+
+
+def measure_reference(args, name, storage, world, headline):
+    """mach's kernel on one workload: float32 / complex64 input (int16 widened exactly, times
+    its scale), one launch + cudaDeviceSynchronize per transmit, into a zeroed output."""
+    from oracle import machref
+
+    frames, side = (args.frames, args.side) if headline else (None, None)
+    w = make_workload(name, frames, side)
+    storage = storage or w.storage
     ch = w.channel
     if ch.dtype == torch.int16:
         ch = ch.to(torch.float32) * w.channel_scale
@@ -823,7 +966,7 @@ def run_reference(args, world, rank, local):
         machref.beamform_device(ch_ptrs, rx.data_ptr(), scan.data_ptr(), arr_ptrs, out.data_ptr(), is_complex=is_c,
                                 n_rx=w.n_rx, n_samples=w.n_samples, n_vox=w.n_vox, n_frames=w.n_frames, **p)
 
-    clocks = ClockSampler(local)
+    clocks = ClockSampler(torch.cuda.current_device())
     clocks.start()
     for _ in range(args.warmup):
         step()
@@ -837,25 +980,21 @@ def run_reference(args, world, rank, local):
         lat.append((time.perf_counter() - s) * 1e3)
     dt = time.perf_counter() - t0
     clock_info = clocks.stop()
-    line = dict(base)
-    line.update({
-        "value": w.points * args.steps / dt,
-        "ms_per_step": dt / args.steps * 1e3,
-        "scaling": "weak",
-        "vs_baseline": None,
-        "dtype": "f32",
+    line = {
+        "metric": METRIC, "value": w.points * args.steps / dt, "unit": "points/s", "impl": "reference",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded simulation of the configuration; no public dataset offline)",
-        "config": {"workload": f"{args.workload}: {WORKLOAD_DESC[args.workload]}",
-                   "storage": "c64" if is_c else "f32", "n_tx": w.n_tx, "n_rx": w.n_rx, "n_samples": w.n_samples,
-                   "n_frames": w.n_frames, "n_vox": w.n_vox, "points_per_step": w.points,
-                   "l2": "inputs larger than L2, no flush",
-                   "parallelism": "rank 0 only"},
+        "config": workload_config(name, w, storage, world),
         "reference": "mach 0.1.3 src/mach/kernel.cu compiled for sm_100a from its unmodified source; one launch + "
-                     "cudaDeviceSynchronize per transmit into a zeroed complex64/float32 out (mach.experimental loop)",
+                     "cudaDeviceSynchronize per transmit into a zeroed complex64/float32 out (mach.experimental loop); "
+                     "rank 0 only",
+        "reference_input": "complex64" if is_c else ("float32 (int16 samples x scale, exact)"
+                                                     if w.storage == "i16" else "float32"),
         "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
         "clocks": clock_info,
         "gpu_launches": w.n_tx * args.steps,
-    })
+    }
     if not args.no_e2e:
         ch_h = ch.cpu().pin_memory()
         rx_h, scan_h = w.rx_coords_m, w.scan_coords_m
@@ -877,9 +1016,15 @@ def run_reference(args, world, rank, local):
         dt = time.perf_counter() - t0
         per_tx = ch_np[0].nbytes + arr_h[0].nbytes + rx_h.nbytes + scan_h.nbytes
         line["e2e"] = {"value": w.points * args.steps / dt, "unit": "points/s",
-                       "h2d_bytes_per_step": int(per_tx * w.n_tx), "d2h_bytes_per_step": int(out_h.numel() * 8 if is_c else out_h.numel() * 4),
+                       "h2d_bytes_per_step": int(per_tx * w.n_tx),
+                       "d2h_bytes_per_step": int(out_h.numel() * 8 if is_c else out_h.numel() * 4),
                        "ms_per_step": dt / args.steps * 1e3,
                        "api": "mach's binding with host arrays per transmit (its CPU staging path), device out"}
+        del ch_h, out_h, ch_np
+    del ch, out, rx, scan, arr
+    w.channel = None
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
     return line
 
 

@@ -12,6 +12,14 @@
  * last failure on the calling thread is available from mach_b200_last_error().
  * No function terminates the process (mach's helper_cuda.h exits on CUDA errors).
  *
+ * Kernels that wait on shared-memory barriers (staged and ensemble families) give up after
+ * a bounded time and set one status word per device; a synchronous call reads and clears it
+ * and fails with MACH_B200_ERR_CUDA.  The word is shared by all calls on a device, so a
+ * timeout in an asynchronous call can be reported by the next synchronous call on any
+ * stream of that device.  Temporary device buffers (host staging, work counters) come from
+ * a memory pool of the library's own (at most 2 GiB of freed memory kept per device); the
+ * process's default memory pool is never reconfigured.
+ *
  * Layouts (C order):
  *   channel_data        [n_tx][n_rx][n_samples][n_frames] samples of `storage`
  *   rx_coords_m         [n_rx][3]   float32, metres
@@ -74,6 +82,9 @@ extern "C" {
 #define MACH_B200_KERNEL_WARP 3       /* a warp per voxel over frames, taps read from global memory */
 #define MACH_B200_KERNEL_ENSEMBLE 4   /* lanes = frames of a 32-lane block, voxel-tile sample windows in
                                          tensor memory (many frames; nearest or linear taps) */
+#define MACH_B200_KERNEL_FRAME_LANE 5 /* lanes = frames, a warp walks a run of neighbouring voxels and
+                                         keeps sample rows in registers (many frames; nearest or
+                                         linear taps) */
 
 /*
  * Optional launch options.  Zero-initialise, set struct_size = sizeof(mach_b200_options),
@@ -103,6 +114,12 @@ typedef struct mach_b200_options {
                                 (spherical), time offset (s), unused.  The arrival is the distance of
                                 src/mach/wavefront.py:8-116 divided by the sound speed, plus the
                                 offset, formed in FP64 and rounded to FP32.  Device or host memory. */
+    int32_t frame_slots;     /* frame-lane kernel: columns of 32 lane words (frames) a warp holds, 1, 2
+                                or 4, with runs of 16, 8 or 4 voxels; 0 = automatic */
+    int32_t prefetch;        /* frame-lane kernel: 1 = sample rows loaded straight from global memory;
+                                2 = rows streamed one parameter batch ahead into a shared-memory ring
+                                by bulk copies (needs n_frames x sample bytes a multiple of 16 and a
+                                16-byte aligned channel_data); 0 = automatic (1) */
 } mach_b200_options;
 
 /* Transmit models (mach_b200_options.tx_model). */
@@ -173,13 +190,16 @@ MACH_B200_API int mach_b200_beamform_ex(int32_t storage, const void* channel_dat
  * allocator, or a real-time acquisition loop that cannot risk a pool growing (and stalling)
  * inside a call.  The ensemble kernel's only scratch, one work-item counter per launch, lives
  * in a static device array of the library (64 counters, 256 bytes on every device that loads
- * it) instead of a stream-ordered allocation; the call allocates, copies and frees nothing.
+ * it) instead of a stream-ordered allocation: the call allocates no device memory, creates no
+ * memory pool and changes no pool setting.  Its only copy is the read-back of the library's
+ * 4-byte timeout status word on synchronous calls (and its reset after a timeout).
  * No counterpart in the reference (mach allocates staging buffers and runs one fixed kernel).
  *
- * - Every buffer must be device memory of the current device.  The job must fit the ensemble
- *   kernel (nearest or linear interpolation, 16-byte aligned channel_data, n_frames x sample
- *   bytes a multiple of 16, fewer than 2^31 voxels) and need at most 64 launches, i.e. at most
- *   64 x (2^31 - 1) channel samples; anything else is rejected with MACH_B200_ERR_VALUE.
+ * - Every buffer must be device memory of the current device (host buffers are rejected, as
+ *   they would need staging buffers).  The job must fit the ensemble kernel (nearest or linear
+ *   interpolation, 16-byte aligned channel_data, n_frames x sample bytes a multiple of 16,
+ *   fewer than 2^31 voxels) and need at most 64 launches, i.e. at most 64 x (2^31 - 1)
+ *   channel samples; anything else is rejected with MACH_B200_ERR_VALUE.
  *   It takes an arrivals array only: options->tx_model must be MACH_B200_TX_ARRAYS, since a
  *   wave model is turned into arrivals in a device buffer.
  * - The first call on a device looks up the counters' device address; make that first call
@@ -187,7 +207,8 @@ MACH_B200_API int mach_b200_beamform_ex(int32_t storage, const void* channel_dat
  * - All calls share the counters (each call zeroes the ones it uses on `cuda_stream`), so two
  *   calls whose work overlaps on the GPU (different streams, or MACH_B200_FLAG_ASYNC calls not
  *   yet finished on other streams) race and give wrong images.  Serialise them.
- * - Same arguments, flags and result as mach_b200_beamform_ex.
+ * - Arguments and result as mach_b200_beamform_ex with the ensemble kernel, except that
+ *   MACH_B200_FLAG_POWER_DOPPLER is rejected (this call writes the frames).
  */
 MACH_B200_API int mach_b200_beamform_ensemble_noalloc(int32_t storage, const void* channel_data,
                                 const float* rx_coords_m, const float* scan_coords_m,
@@ -277,6 +298,25 @@ MACH_B200_API int mach_b200_batch_run(mach_b200_batch* batch, const mach_b200_jo
 
 /* Release a batch context (waits for its device work to finish). */
 MACH_B200_API void mach_b200_batch_destroy(mach_b200_batch* batch);
+
+/*
+ * Measurement helper with no counterpart in the reference: launch, on `cuda_stream`, one
+ * kernel that reads `bytes` of the device buffer `buffer` (16-byte aligned, a multiple of 16
+ * bytes) `passes` times with L2-cached, L1-bypassing 16-byte loads, spread over every SM.
+ * Timed with CUDA events around the launch (after one untimed launch), bytes x passes /
+ * time is the L2 read bandwidth when the buffer is smaller than L2: the peak that the gather
+ * kernels' L2 traffic is reported against.  Returns MACH_B200_ERR_VALUE for a host, foreign-
+ * device or misaligned buffer.
+ */
+MACH_B200_API int mach_b200_probe_l2_read(const void* buffer, uint64_t bytes, uint32_t passes, void* cuda_stream);
+
+/*
+ * Diagnostic with no counterpart in the reference: the library's own memory pool on CUDA
+ * device `device` (zeros while the library has not allocated anything there).  *used_high is
+ * the most pool memory in use at once since the last reset, *reserved the memory the pool
+ * holds now.  reset_high != 0 first resets the high-water mark to the memory in use now.
+ */
+MACH_B200_API int mach_b200_pool_stats(int32_t device, int32_t reset_high, uint64_t* used_high, uint64_t* reserved);
 
 /* Message of the last failed call on this thread ("" if none). */
 MACH_B200_API const char* mach_b200_last_error(void);

@@ -4,14 +4,29 @@ Same public surface as mach (src/mach/__init__.py:17-31): ``beamform``, ``kernel
 ``experimental``, ``wavefront``, ``geometry``, ``Array``.  ``import mach_b200 as mach``
 is enough for code written against mach's API.  The beamformer runs in hand-written
 sm_100a CUDA kernels in ``libmach_b200.so`` (C ABI: ``include/mach_b200.h``).
+
+The submodules are imported on first use, so that host-only helpers (``geometry``,
+``wavefront``, ``workloads``) can be used without opening the CUDA library.  The first
+use of anything that beamforms loads the library and raises ``ImportError`` if it is
+missing; there is no fallback.
 """
 
-from mach_b200 import experimental, geometry, kernel, wavefront
-from mach_b200._array_api import Array
-from mach_b200._cuda_impl import InterpolationType
-from mach_b200.kernel import beamform
+from __future__ import annotations
 
-__version__ = "0.1.0"
+import importlib
+
+__version__ = "0.2.0"
+
+# public name -> (submodule, attribute or None for the submodule itself)
+_LAZY = {
+    "Array": ("_array_api", "Array"),
+    "InterpolationType": ("_cuda_impl", "InterpolationType"),
+    "beamform": ("kernel", "beamform"),
+    "experimental": ("experimental", None),
+    "geometry": ("geometry", None),
+    "kernel": ("kernel", None),
+    "wavefront": ("wavefront", None),
+}
 
 __all__ = [
     "Array",
@@ -23,3 +38,18 @@ __all__ = [
     "kernel",
     "wavefront",
 ]
+
+
+def __getattr__(name: str):
+    try:
+        module, attr = _LAZY[name]
+    except KeyError:
+        raise AttributeError(f"module 'mach_b200' has no attribute {name!r}") from None
+    mod = importlib.import_module(f"mach_b200.{module}")
+    value = mod if attr is None else getattr(mod, attr)
+    globals()[name] = value
+    return value
+
+
+def __dir__():
+    return sorted(set(globals()) | set(_LAZY))

@@ -57,14 +57,16 @@ class Options(ctypes.Structure):
         ("tx_model", ctypes.c_int32),
         ("tile_fast", ctypes.c_int32),
         ("tx_params", ctypes.c_void_p),
+        ("frame_slots", ctypes.c_int32),
+        ("prefetch", ctypes.c_int32),
     ]
 
 
-KERNELS = {"auto": 0, "lane_voxel": 1, "staged": 2, "warp": 3, "ensemble": 4}
+KERNELS = {"auto": 0, "lane_voxel": 1, "staged": 2, "warp": 3, "ensemble": 4, "frame_lane": 5}
 
 
 def make_options(flags: int = 0, grid_shape=None, kernel: str | int = 0, tx_chunk: int = 0, window_rows: int = 0,
-                 lanes_per_voxel: int = 0, tile_fast: int = 0) -> Options:
+                 lanes_per_voxel: int = 0, tile_fast: int = 0, frame_slots: int = 0, prefetch: int = 0) -> Options:
     o = Options()
     o.struct_size = ctypes.sizeof(Options)
     o.flags = int(flags)
@@ -76,6 +78,8 @@ def make_options(flags: int = 0, grid_shape=None, kernel: str | int = 0, tx_chun
     o.window_rows = int(window_rows)
     o.lanes_per_voxel = int(lanes_per_voxel)
     o.tile_fast = int(tile_fast)
+    o.frame_slots = int(frame_slots)
+    o.prefetch = int(prefetch)
     return o
 
 
@@ -90,6 +94,8 @@ _lib.mach_b200_hilbert.argtypes = [_I32, _P, _I32, _I32, _P, _U32, _U32, _U32, _
 _lib.mach_b200_hilbert.restype = ctypes.c_int
 LAYOUT_CHANNEL = 0
 LAYOUT_ACQUISITION = 1
+_lib.mach_b200_probe_l2_read.argtypes = [_P, _U64, _U32, _P]
+_lib.mach_b200_probe_l2_read.restype = ctypes.c_int
 _lib.mach_b200_last_error.restype = ctypes.c_char_p
 _lib.mach_b200_nvcc_version.restype = ctypes.c_char_p
 _lib.mach_b200_version.restype = ctypes.c_char_p
@@ -120,6 +126,13 @@ class InterpolationType(enum.IntEnum):
 NearestNeighbor = InterpolationType.NearestNeighbor
 Linear = InterpolationType.Linear
 Quadratic = InterpolationType.Quadratic
+
+
+def probe_l2_read(ptr: int, nbytes: int, passes: int, stream: int = 0) -> None:
+    """Launch the L2 read-bandwidth probe over a device buffer (``mach_b200_probe_l2_read``)."""
+    rc = _lib.mach_b200_probe_l2_read(ptr, nbytes, passes, stream)
+    if rc != 0:
+        raise RuntimeError(f"mach_b200_probe_l2_read failed with code {rc}")
 
 
 def launch_count() -> int:

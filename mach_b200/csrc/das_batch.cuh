@@ -9,6 +9,7 @@
 // transmit counts share the launch; the GPU stays full until the last item.
 #pragma once
 
+#include "das_frame_lane.cuh"
 #include "das_lane_voxel.cuh"
 #include "das_staged.cuh"
 
@@ -18,7 +19,8 @@ struct alignas(64) BatchJob {
     CUtensorMap map;  // staged family: TMA view of this job's channel data (64-byte aligned)
     DasArgs a;
     StagedArgs st;
-    int32_t tiles;   // spatial tiles
+    FrameLaneArgs fl;  // frame-lane family: run mapping and ring layout
+    int32_t tiles;   // spatial tiles (frame-lane family: CTA blocks)
     int32_t chunks;  // frame chunks per tile (staged family), 1 otherwise
 };
 
@@ -95,6 +97,24 @@ __global__ void __launch_bounds__(kStagedThreads, 3)
         const int tile = static_cast<int>(s_local / chunks);
         const int chunk = static_cast<int>(s_local - static_cast<int64_t>(tile) * chunks);
         if (!staged_tile<S, INTERP, LV>(s_args, s_st, &jobs[s_job].map, tile, chunk, smem)) return;
+    }
+}
+
+template <int S, int INTERP, int J, bool SPLIT, bool RING>
+__global__ void __launch_bounds__(kFrameLaneThreads, 4)
+    das_frame_lane_persistent(const BatchHeader* __restrict__ hdr, const BatchJob* __restrict__ jobs,
+                              const int64_t* __restrict__ item_begin, unsigned long long* counter) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    __shared__ DasArgs s_args;
+    __shared__ FrameLaneArgs s_fl;
+    __shared__ int s_job;
+    __shared__ int64_t s_local;
+    int cursor = 0;
+    while (next_item(hdr, item_begin, counter, cursor, &s_job, &s_local)) {
+        copy_words(&s_args, &jobs[s_job].a);
+        copy_words(&s_fl, &jobs[s_job].fl);
+        __syncthreads();
+        frame_lane_block<S, INTERP, J, 16 / J, SPLIT, RING>(s_args, s_fl, s_local, smem_raw);
     }
 }
 

@@ -10,4 +10,7 @@ template cudaError_t launch_lane_voxel_persistent<kCBF16>(int, int, bool, const 
 template cudaError_t launch_staged_persistent<kCBF16>(int, int, const PersistentLaunch&, cudaStream_t);
 template cudaError_t launch_das_ensemble<kCBF16>(const DasArgs&, const StagedArgs&, const EnsembleArgs&,
                                                const CUtensorMap&, int, size_t, cudaStream_t);
+template cudaError_t launch_das_frame_lane<kCBF16>(const DasArgs&, const FrameLaneArgs&, int, const LaunchPlan&,
+                                                cudaStream_t);
+template cudaError_t launch_frame_lane_persistent<kCBF16>(int, int, bool, const PersistentLaunch&, cudaStream_t);
 }  // namespace mach_b200

@@ -159,7 +159,7 @@ __device__ __forceinline__ float2 widen_i16x2(unsigned w) {
     const unsigned u = w ^ 0x80008000u;
     const float lo = __uint_as_float(__byte_perm(u, 0x4B000000u, 0x7610));
     const float hi = __uint_as_float(__byte_perm(u, 0x4B000000u, 0x7632));
-    return make_float2(__fsub_rn(lo, 8421376.0f), __fsub_rn(hi, 8421376.0f));
+    return __fadd2_rn(make_float2(lo, hi), make_float2(-8421376.0f, -8421376.0f));  // exact
 }
 template <>
 __device__ __forceinline__ void widen8<kCI16>(uint2 r, float2* o) {
@@ -466,6 +466,27 @@ __device__ __forceinline__ void lane_voxel_tile(const DasArgs& a, int64_t tile, 
                         }
                     }
                     const T* p = channel + (row + tp.idx * fstride + f0);
+                    if constexpr (kVec && !kCplx && INTERP != kQuadratic) {
+                        // Real frames in pairs: the interpolation weights folded into the
+                        // apodisation weight, acc += (1 - t) w a + t w b in packed FP32x2.
+                        float2 va[kAcc];
+                        load_frames<S, NF>(p, va);
+                        if constexpr (INTERP == kLinear) {
+                            float2 vb[kAcc];
+                            load_frames<S, NF>(p + tp.step * fstride, vb);
+                            const float wb = __fmul_rn(tp.w0, cw);
+                            const float wa = __fsub_rn(cw, wb);
+#pragma unroll
+                            for (int q = 0; q < kAcc; ++q) {
+                                acc[q] = __ffma2_rn(make_float2(wa, wa), va[q], acc[q]);
+                                acc[q] = __ffma2_rn(make_float2(wb, wb), vb[q], acc[q]);
+                            }
+                        } else {
+#pragma unroll
+                            for (int q = 0; q < kAcc; ++q) acc[q] = __ffma2_rn(make_float2(cw, cw), va[q], acc[q]);
+                        }
+                        continue;
+                    }
                     if constexpr (kVec) {
                         float2 va[kAcc], vb[kAcc], vc[kAcc];
                         if constexpr (INTERP == kNearest) {
@@ -580,13 +601,15 @@ struct PairRx {
     float w;       // apodisation weight x storage scale
 };
 
+// SM: delay mode known at compile time (0 reference, 1 split), or -1 to read a.split.
+template <int SM = -1>
 __device__ __forceinline__ bool pair_receive(const DasArgs& a, float ex, float ey, float ez, float vx, float vy,
                                              float vz, float radius, float radius_sq, PairRx& rx) {
     const float dx = __fsub_rn(ex, vx);
     const float dy = __fsub_rn(ey, vy);
     const float dz = __fsub_rn(ez, vz);
     const float h2 = __fmaf_rn(dx, dx, __fmul_rn(dy, dy));
-    if (a.split) {
+    if (SM < 0 ? a.split != 0 : SM != 0) {
         const double ddx = static_cast<double>(ex) - vx, ddy = static_cast<double>(ey) - vy,
                      ddz = static_cast<double>(ez) - vz;
         const double d = sqrt(fma(ddx, ddx, fma(ddy, ddy, ddz * ddz)));
@@ -603,13 +626,13 @@ __device__ __forceinline__ bool pair_receive(const DasArgs& a, float ex, float e
 
 // Transmit part of one point: tap index, interpolation parameter (linear: t, quadratic: x
 // from the centre tap) and the weighted phasor.  Returns false when the point is skipped.
-template <int INTERP, bool CPLX>
+template <int INTERP, bool CPLX, int SM = -1>
 __device__ __forceinline__ bool point_taps(const DasArgs& a, const PairRx& rx, float txa, int& idx, float& w,
                                            float& cw, float& sw) {
     TapPosition tp{};
     float sn = 0.f, cs = 1.f;
     bool ok;
-    if (a.split) {
+    if (SM < 0 ? a.split != 0 : SM != 0) {
         const SplitPos tx = split_position((static_cast<double>(txa) - a.t0_d) * a.fs_d);
         int base = tx.base + rx.pos.base;
         float frac = __fadd_rn(tx.frac, rx.pos.frac);

@@ -5,6 +5,7 @@
 
 #include "das_batch.cuh"
 #include "das_ensemble.cuh"
+#include "das_frame_lane.cuh"
 #include "das_gather.cuh"
 #include "das_lane_voxel.cuh"
 #include "das_staged.cuh"
@@ -20,6 +21,7 @@ enum KernelKind : int {
     kKindLaneVoxel16 = 5,  // das_lane_voxel_kernel, exactly 16 frames loaded as 16-byte vectors
     kKindEnsemble = 6,     // das_ensemble_kernel, windows in tensor memory, lanes = frames
     kKindLaneVoxel8 = 7,   // das_lane_voxel_kernel, chunks of 8 frames (grid.y) of a longer ensemble
+    kKindFrameLane = 8,    // das_frame_lane_kernel, lanes = frames, rows reused along voxel runs
 };
 
 struct LaunchPlan {
@@ -34,6 +36,8 @@ struct LaunchPlan {
     int map_wlog;
     int64_t map_outer;
     int frame_chunks;   // lane-voxel 8-frame chunks per tile (DasArgs::frame_chunks)
+    int frame_slots;    // frame-lane kernel: J, lane-word columns per warp (1, 2 or 4)
+    int run_voxels;     // frame-lane kernel: G, voxels per warp run (J * G = 16)
 };
 
 // Opt a kernel into more than 48 KB of dynamic shared memory (once per instance is enough,
@@ -119,6 +123,38 @@ cudaError_t launch_das(const DasArgs& a, int interp, const LaunchPlan& p, cudaSt
     return cudaGetLastError();
 }
 
+// Frame-lane kernel: (J, G) pairs with J * G = 16 (64 accumulator registers for complex storage)
+// with the shared-memory row ring; direct row loads with (4, 4).
+template <int S, int I, int J, bool SPLIT, bool RING>
+cudaError_t launch_frame_lane_k(const DasArgs& a, const FrameLaneArgs& fl, const LaunchPlan& p, cudaStream_t stream) {
+    auto kernel = das_frame_lane_kernel<S, I, J, 16 / J, SPLIT, RING>;
+    const cudaError_t e = allow_smem(kernel, p.smem);
+    if (e != cudaSuccess) return e;
+    kernel<<<p.grid, p.block, p.smem, stream>>>(a, fl);
+    return cudaGetLastError();
+}
+
+template <int S, int I, bool SPLIT>
+cudaError_t launch_frame_lane_i(const DasArgs& a, const FrameLaneArgs& fl, const LaunchPlan& p, cudaStream_t stream) {
+    if (fl.ring_slots == 0) return launch_frame_lane_k<S, I, 4, SPLIT, false>(a, fl, p, stream);
+    switch (p.frame_slots) {
+        case 1: return launch_frame_lane_k<S, I, 1, SPLIT, true>(a, fl, p, stream);
+        case 2: return launch_frame_lane_k<S, I, 2, SPLIT, true>(a, fl, p, stream);
+        default: return launch_frame_lane_k<S, I, 4, SPLIT, true>(a, fl, p, stream);
+    }
+}
+
+template <int S>
+cudaError_t launch_das_frame_lane(const DasArgs& a, const FrameLaneArgs& fl, int interp, const LaunchPlan& p,
+                                  cudaStream_t stream) {
+    if (interp == kNearest) {
+        return a.split ? launch_frame_lane_i<S, kNearest, true>(a, fl, p, stream)
+                       : launch_frame_lane_i<S, kNearest, false>(a, fl, p, stream);
+    }
+    return a.split ? launch_frame_lane_i<S, kLinear, true>(a, fl, p, stream)
+                   : launch_frame_lane_i<S, kLinear, false>(a, fl, p, stream);
+}
+
 // ---------------------------------------------------------------- persistent batch launches
 
 struct PersistentLaunch {
@@ -167,6 +203,28 @@ cudaError_t launch_lane_voxel_persistent(int interp, int frame_class, bool split
     }
 #undef MACH_B200_PLV_NF
 #undef MACH_B200_PLV
+}
+
+// Frame-lane family: variant = J (1, 2, 4) with the row ring, 100 + 4 for direct loads.
+template <int S>
+cudaError_t launch_frame_lane_persistent(int interp, int variant, bool split, const PersistentLaunch& pl,
+                                         cudaStream_t stream) {
+#define MACH_B200_PFL(I, J, R)                                                                                      \
+    return split ? launch_persistent(das_frame_lane_persistent<S, I, J, true, R>, kFrameLaneThreads, pl, stream) \
+                 : launch_persistent(das_frame_lane_persistent<S, I, J, false, R>, kFrameLaneThreads, pl, stream)
+#define MACH_B200_PFL_V(I)              \
+    switch (variant) {                  \
+        case 1: MACH_B200_PFL(I, 1, true); \
+        case 2: MACH_B200_PFL(I, 2, true); \
+        case 4: MACH_B200_PFL(I, 4, true); \
+        default: MACH_B200_PFL(I, 4, false); \
+    }
+    if (interp == kNearest) {
+        MACH_B200_PFL_V(kNearest)
+    }
+    MACH_B200_PFL_V(kLinear)
+#undef MACH_B200_PFL_V
+#undef MACH_B200_PFL
 }
 
 template <int S>

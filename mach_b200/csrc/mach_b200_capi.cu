@@ -14,6 +14,7 @@
 #include <vector>
 
 #include "das_launch.cuh"
+#include "das_split.h"
 #include "mach_b200.h"
 
 #ifndef MACH_B200_NVCC_VERSION
@@ -26,7 +27,17 @@ namespace mach_b200 {
 #define MACH_B200_EXTERN(S)                                                                                  \
     extern template cudaError_t launch_das<S>(const DasArgs&, int, const LaunchPlan&, cudaStream_t);         \
     extern template cudaError_t launch_das_staged<S>(const DasArgs&, const StagedArgs&, const CUtensorMap&, \
-                                                     int, const LaunchPlan&, cudaStream_t);
+                                                     int, const LaunchPlan&, cudaStream_t);                 \
+    extern template cudaError_t launch_das_frame_lane<S>(const DasArgs&, const FrameLaneArgs&, int,         \
+                                                         const LaunchPlan&, cudaStream_t);                   \
+    extern template cudaError_t launch_das_ensemble<S>(const DasArgs&, const StagedArgs&,                  \
+                                                       const EnsembleArgs&, const CUtensorMap&, int, size_t,  \
+                                                       cudaStream_t);                                         \
+    extern template cudaError_t launch_lane_voxel_persistent<S>(int, int, bool, const PersistentLaunch&,    \
+                                                                cudaStream_t);                               \
+    extern template cudaError_t launch_staged_persistent<S>(int, int, const PersistentLaunch&, cudaStream_t); \
+    extern template cudaError_t launch_frame_lane_persistent<S>(int, int, bool, const PersistentLaunch&,    \
+                                                                cudaStream_t);
 MACH_B200_EXTERN(kF32)
 MACH_B200_EXTERN(kC64)
 MACH_B200_EXTERN(kF16)
@@ -118,31 +129,54 @@ struct DeviceState {
     std::once_flag once;
     cudaError_t init_error = cudaSuccess;
     int* status = nullptr;  // device address of g_mach_b200_status
+    std::once_flag pool_once;
+    cudaError_t pool_error = cudaSuccess;
+    std::atomic<cudaMemPool_t> pool{nullptr};  // the library's own stream-ordered pool for staging buffers
 };
 DeviceState g_devices[kMaxDevices];
 
-// First call on a device (that device current): look up the status word and keep the
-// stream-ordered pool's memory cached between calls.
+// First call on a device (that device current): look up the status word.  Nothing else of the
+// process's CUDA state is touched (its default memory pool keeps its settings).
 int device_state(int device, DeviceState** out) {
     if (device < 0 || device >= kMaxDevices) return fail(MACH_B200_ERR_DEVICE, "device %d out of range", device);
     DeviceState& d = g_devices[device];
-    std::call_once(d.once, [&d, device]() {
+    std::call_once(d.once, [&d]() {
         void* p = nullptr;
         d.init_error = cudaGetSymbolAddress(&p, g_mach_b200_status);
         d.status = static_cast<int*>(p);
-        if (d.init_error == cudaSuccess) {
-            cudaMemPool_t pool;
-            if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
-                uint64_t keep = UINT64_MAX;
-                cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
-            }
-        }
     });
     if (d.init_error != cudaSuccess) {
         return fail(MACH_B200_ERR_CUDA, "device setup failed: %s", cudaGetErrorString(d.init_error));
     }
     *out = &d;
     return MACH_B200_OK;
+}
+
+// Memory pool of the library's temporary device buffers on `device`, created on first use.
+// It keeps up to kPoolKeepBytes of freed memory cached between calls (host-staged jobs
+// allocate the same buffers call after call); beyond that, freed memory goes back to the
+// driver at the next synchronisation.
+constexpr uint64_t kPoolKeepBytes = uint64_t{2} << 30;
+
+cudaError_t library_pool(int device, cudaMemPool_t* pool) {
+    if (device < 0 || device >= kMaxDevices) return cudaErrorInvalidDevice;
+    DeviceState& d = g_devices[device];
+    std::call_once(d.pool_once, [&d, device]() {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.handleTypes = cudaMemHandleTypeNone;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = device;
+        cudaMemPool_t created = nullptr;
+        d.pool_error = cudaMemPoolCreate(&created, &props);
+        if (d.pool_error == cudaSuccess) {
+            uint64_t keep = kPoolKeepBytes;
+            d.pool_error = cudaMemPoolSetAttribute(created, cudaMemPoolAttrReleaseThreshold, &keep);
+            d.pool.store(created);
+        }
+    });
+    *pool = d.pool.load();
+    return d.pool_error;
 }
 
 PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
@@ -167,8 +201,10 @@ struct Plan {
     LaunchPlan lp{};
     StagedArgs st{};
     EnsembleArgs ea{};
+    FrameLaneArgs fl{};
     bool staged = false;
     bool ensemble = false;
+    bool frame_lane = false;
 };
 
 int next_pow2(int x) {
@@ -260,8 +296,94 @@ bool plan_ensemble(int storage, int interp, uint64_t n_vox, uint32_t n_frames, u
     return true;
 }
 
+// Frame-lane kernel plan (lanes = frames, sample rows reused in registers along runs of
+// neighbouring voxels), or false when the job does not meet its conditions: nearest / linear
+// taps, an even frame count for real storage, lane words aligned, at least one full column of
+// 32 lane words per sample row.  Runs lie along the mid axis of a 3-D grid and the slow axis of
+// a 2-D one (the lateral axes, where delays change least from voxel to voxel); without a grid
+// they are runs of consecutive voxels.
+bool plan_frame_lane(int storage, int interp, uint64_t n_vox, uint32_t n_frames, const void* channel,
+                     bool channel_on_device, const mach_b200_options& o, Plan& p) {
+    const bool cplx = (storage & 1) != 0;
+    const int word_bytes = (storage == kC64 || storage == kF32) ? 8 : 4;
+    if (interp != kNearest && interp != kLinear) return false;
+    if (n_vox == 0 || n_frames == 0 || (!cplx && n_frames % 2 != 0)) return false;
+    if (channel_on_device && reinterpret_cast<uintptr_t>(channel) % word_bytes != 0) return false;
+    const int64_t words = cplx ? n_frames : n_frames / 2;
+    if (words < 32) return false;
+    int J = o.frame_slots;
+    if (J != 1 && J != 2 && J != 4) J = words <= 32 ? 1 : (words <= 64 ? 2 : 4);
+    // Ring mode (asked for with prefetch = 2; measured slower than direct loads on B200) needs
+    // 16-byte aligned rows for its bulk copies; the direct mode runs (J, G) = (4, 4).
+    const bool ring_ok = o.prefetch == 2 && (words * word_bytes) % 16 == 0 &&
+                         (!channel_on_device || reinterpret_cast<uintptr_t>(channel) % 16 == 0);
+    const int coef = cplx ? 2 : 1;
+    int slots = 0;
+    if (ring_ok) {
+        // Row buffers per warp: the most (a power of two, 4..16) that keep a CTA of four warps
+        // within 56 KB, so that four CTAs fit an SM.
+        const int slot_bytes = 32 * J * word_bytes;
+        for (int k = 16; k >= 4; k >>= 1) {
+            const int wb = coef == 2 ? frame_lane_warp_bytes<2>(k, slot_bytes) : frame_lane_warp_bytes<1>(k, slot_bytes);
+            if (kFrameLaneWarps * wb <= 56 * 1024) {
+                slots = k;
+                break;
+            }
+        }
+    }
+    if (slots == 0) {
+        J = 4;
+    }
+    const int G = 16 / J;
+    FrameLaneArgs& fl = p.fl;
+    fl.slot_bytes = 32 * J * word_bytes;
+    fl.ring_slots = slots;
+    fl.ring_log2 = slots == 16 ? 4 : (slots == 8 ? 3 : (slots == 4 ? 2 : 0));
+    fl.warp_bytes = coef == 2 ? frame_lane_warp_bytes<2>(slots, fl.slot_bytes)
+                              : frame_lane_warp_bytes<1>(slots, fl.slot_bytes);
+    if (grid_matches(o, n_vox)) {
+        const int64_t slow = o.grid_shape[0], mid = o.grid_shape[1], fast = o.grid_shape[2];
+        fl.n_fast = fast;
+        fl.run_stride = fast;
+        if (mid > 1) {
+            fl.run_len = mid;
+            fl.n_across = slow;
+            fl.across_stride = mid * fast;
+        } else {
+            fl.run_len = slow;
+            fl.n_across = 1;
+            fl.across_stride = 0;
+        }
+    } else {
+        fl.run_len = static_cast<int64_t>(n_vox);
+        fl.run_stride = 1;
+        fl.n_across = 1;
+        fl.across_stride = 0;
+        fl.n_fast = 1;
+    }
+    fl.runs_per_line = (fl.run_len + G - 1) / G;
+    fl.n_runs = fl.runs_per_line * fl.n_across * fl.n_fast;
+    fl.words = static_cast<int32_t>(words);
+    fl.n_chunks = static_cast<int32_t>((words + 32 * J - 1) / (32 * J));
+    const int64_t ctas = (fl.n_runs + kFrameLaneWarps - 1) / kFrameLaneWarps * fl.n_chunks;
+    if (ctas > 0x7fffffffll) return false;
+    p.frame_lane = true;
+    p.lp.kind = kKindFrameLane;
+    p.lp.frame_slots = J;
+    p.lp.run_voxels = G;
+    p.lp.block = dim3(kFrameLaneThreads, 1, 1);
+    p.lp.grid = dim3(static_cast<unsigned>(ctas), 1, 1);
+    p.lp.passes = 1;
+    p.lp.tx_chunk = 1;
+    p.lp.lanes_per_voxel = 32;
+    p.lp.smem = static_cast<size_t>(kFrameLaneWarps) * fl.warp_bytes;
+    return true;
+}
+
+// interp < 0: a caller that runs neither the frame-lane nor the ensemble kernel; batch: a
+// persistent batch, which runs the frame-lane kernel but not the ensemble kernel.
 Plan plan_launch(int storage, uint64_t n_vox, uint32_t n_frames, uint32_t n_tx, const void* channel,
-                 bool channel_on_device, const mach_b200_options& o, int interp = -1) {
+                 bool channel_on_device, const mach_b200_options& o, int interp = -1, bool batch = false) {
     Plan p;
     const int esz = static_cast<int>(storage_bytes(storage));
     const int vf = 8 / esz;
@@ -278,9 +400,15 @@ Plan plan_launch(int storage, uint64_t n_vox, uint32_t n_frames, uint32_t n_tx, 
     if (kind == MACH_B200_KERNEL_AUTO && lane8_ok && esz == 4 && (storage & 1) && grid_matches(o, n_vox)) {
         kind = MACH_B200_KERNEL_LANE_VOXEL;
     }
-    // Ensemble kernel: asked for, or automatic for many frames on a known voxel grid
-    // (interp < 0: a caller that cannot run it, e.g. a batch).
-    if (interp >= 0) {
+    // Frame-lane kernel: when asked for (measured on B200, the ensemble kernel and the 8-frame
+    // chunks stay faster on the 200-frame Doppler job; the autotuner times all three).
+    if (interp >= 0 && kind == MACH_B200_KERNEL_FRAME_LANE) {
+        if (plan_frame_lane(storage, interp, n_vox, n_frames, channel, channel_on_device, o, p)) return p;
+        p = Plan{};
+    }
+    if (kind == MACH_B200_KERNEL_FRAME_LANE) kind = MACH_B200_KERNEL_AUTO;
+    // Ensemble kernel: asked for, or automatic for many frames on a known voxel grid.
+    if (interp >= 0 && !batch) {
         const bool many = n_frames >= ((storage & 1) ? 32u : 64u);
         if (kind == MACH_B200_KERNEL_ENSEMBLE ||
             (kind == MACH_B200_KERNEL_AUTO && many && grid_matches(o, n_vox))) {
@@ -427,6 +555,21 @@ cudaError_t dispatch(int storage, const DasArgs& a, int interp, const Plan& plan
     case S:                                                                             \
         return plan.staged ? launch_das_staged<S>(a, plan.st, map, interp, plan.lp, st) \
                            : launch_das<S>(a, interp, plan.lp, st);
+    if (plan.frame_lane) {
+#define MACH_B200_FCASE(S) \
+    case S: return launch_das_frame_lane<S>(a, plan.fl, interp, plan.lp, st);
+        switch (storage) {
+            MACH_B200_FCASE(kF32)
+            MACH_B200_FCASE(kC64)
+            MACH_B200_FCASE(kF16)
+            MACH_B200_FCASE(kCF16)
+            MACH_B200_FCASE(kBF16)
+            MACH_B200_FCASE(kCBF16)
+            MACH_B200_FCASE(kI16)
+            default: return launch_das_frame_lane<kCI16>(a, plan.fl, interp, plan.lp, st);
+        }
+#undef MACH_B200_FCASE
+    }
     if (plan.ensemble) {
 #define MACH_B200_ECASE(S) \
     case S: return launch_das_ensemble<S>(a, plan.st, plan.ea, map, interp, plan.lp.smem, st);
@@ -466,7 +609,12 @@ struct DeviceBuffer {
     DeviceBuffer& operator=(const DeviceBuffer&) = delete;
     cudaError_t alloc(size_t bytes, cudaStream_t st) {
         stream = st;
-        return cudaMallocAsync(&ptr, bytes ? bytes : 1, st);
+        int device = 0;
+        cudaMemPool_t pool = nullptr;
+        cudaError_t e = cudaGetDevice(&device);
+        if (e == cudaSuccess) e = library_pool(device, &pool);
+        if (e != cudaSuccess) return e;
+        return cudaMallocFromPoolAsync(&ptr, bytes ? bytes : 1, pool, st);
     }
     ~DeviceBuffer() {
         if (ptr) cudaFreeAsync(ptr, stream);
@@ -478,25 +626,22 @@ struct DeviceBuffer {
 int dispatch_split(int storage, DasArgs a, int interp, const Plan& plan, cudaStream_t st) {
     const size_t esz = storage_bytes(storage);
     const int64_t per_tx = static_cast<int64_t>(a.n_rx) * a.row_stride;
-    const int64_t max_tx = std::max<int64_t>(1, ((int64_t{1} << 31) - 1) / std::max<int64_t>(per_tx, 1));
     const char* ch = static_cast<const char*>(a.channel);
-    const float* arr = a.arrivals;
     const int total = a.n_tx;
+    const TransmitSplit split = split_transmits(per_tx, total);
     // Ensemble launches take work items from a zeroed device counter (one per launch).
-    const int n_launch = static_cast<int>((std::max(total, 1) + max_tx - 1) / max_tx);
     DeviceBuffer counters;
     Plan pl = plan;
     if (plan.ensemble) {
-        MACH_B200_CUDA_TRY(counters.alloc(sizeof(int) * n_launch, st));
-        MACH_B200_CUDA_TRY(cudaMemsetAsync(counters.ptr, 0, sizeof(int) * n_launch, st));
+        MACH_B200_CUDA_TRY(counters.alloc(sizeof(int) * static_cast<size_t>(split.n_launch), st));
+        MACH_B200_CUDA_TRY(cudaMemsetAsync(counters.ptr, 0, sizeof(int) * static_cast<size_t>(split.n_launch), st));
     }
-    int launch = 0;
-    int t0 = 0;
-    do {
+    for (int64_t k = 0; k < split.n_launch; ++k) {
+        const int64_t t0 = launch_first_tx(split, k);
         DasArgs b = a;
-        b.n_tx = static_cast<int32_t>(std::min<int64_t>(max_tx, total - t0));
-        b.channel = ch + static_cast<size_t>(t0) * per_tx * esz;
-        b.arrivals = arr + static_cast<int64_t>(t0) * a.n_vox;
+        b.n_tx = static_cast<int32_t>(launch_tx_count(split, total, k));
+        b.channel = ch + static_cast<size_t>(t0) * static_cast<size_t>(per_tx) * esz;
+        b.arrivals = a.arrivals + t0 * a.n_vox;
         b.accumulate = t0 == 0 ? a.accumulate : 1;
         CUtensorMap map;
         std::memset(&map, 0, sizeof(map));
@@ -507,11 +652,9 @@ int dispatch_split(int storage, DasArgs a, int interp, const Plan& plan, cudaStr
                                               plan.st.window_rows);
             if (rc) return rc;
         }
-        if (plan.ensemble) pl.ea.counter = static_cast<int*>(counters.ptr) + launch;
+        if (plan.ensemble) pl.ea.counter = static_cast<int*>(counters.ptr) + k;
         MACH_B200_CUDA_TRY(dispatch(storage, b, interp, pl, map, st));
-        ++launch;
-        t0 += static_cast<int>(max_tx);
-    } while (t0 < total);
+    }
     return MACH_B200_OK;
 }
 
@@ -669,6 +812,7 @@ int compound_impl(int32_t storage, const void* channel_data, const float* rx_coo
     const bool overwrite = (flags & MACH_B200_FLAG_OVERWRITE) != 0u || r_out != kOnDevice;
     Plan plan = plan_launch(storage, n_scan, n_frames, n_tx, channel_data, r_ch == kOnDevice, opt, interp_type);
     plan.st.status = dev->status;
+    plan.fl.status = dev->status;
     a.frame_passes = plan.lp.passes;
     a.tx_chunk = plan.lp.tx_chunk;
     a.map_fast = plan.lp.map_fast;
@@ -687,7 +831,7 @@ int compound_impl(int32_t storage, const void* channel_data, const float* rx_coo
         if ((rc = dispatch_split(storage, a, interp_type, plan, stream))) return rc;
         if (!(flags & MACH_B200_FLAG_ASYNC)) {
             MACH_B200_CUDA_TRY(cudaStreamSynchronize(stream));
-            if (plan.staged || plan.ensemble) return check_status(dev, stream);
+            if (plan.staged || plan.ensemble || plan.frame_lane) return check_status(dev, stream);
         }
         return MACH_B200_OK;
     }
@@ -780,7 +924,7 @@ int compound_impl(int32_t storage, const void* channel_data, const float* rx_coo
     }
     // Host buffers are in use until the stream drains: always synchronous here.
     MACH_B200_CUDA_TRY(cudaStreamSynchronize(stream));
-    if (plan.staged || plan.ensemble) return check_status(dev, stream);
+    if (plan.staged || plan.ensemble || plan.frame_lane) return check_status(dev, stream);
     return MACH_B200_OK;
 }
 
@@ -883,12 +1027,13 @@ int power_impl(int32_t storage, const void* channel_data, const float* rx_coords
     const bool cplx = (storage & 1) != 0;
     const size_t power_bytes = static_cast<size_t>(n_scan) * sizeof(float);
 
-    // ---- fused: the ensemble kernel adds |x|^2 of each frame block into out
+    // ---- fused: the ensemble / frame-lane kernel adds |x|^2 of each frame block into out
     if (all_device && need_channel) {
         Plan plan = plan_launch(storage, n_scan, n_frames, n_tx, channel_data, true, opt, interp_type);
         const int64_t per_tx = static_cast<int64_t>(n_rx) * n_samples * n_frames;
-        if (plan.ensemble && per_tx * n_tx < (int64_t{1} << 31)) {
+        if ((plan.ensemble || plan.frame_lane) && per_tx * n_tx < (int64_t{1} << 31)) {
             plan.st.status = dev->status;
+            plan.fl.status = dev->status;
             DasArgs a = make_args(rx_coords_m, scan_coords_m, n_scan, n_rx, n_samples, n_frames, f_number, rx_start_s,
                                   sampling_freq_hz, sound_speed_m_s, modulation_freq_hz, tukey_alpha, channel_scale,
                                   cplx, flags);
@@ -1165,24 +1310,23 @@ int noalloc_impl(int32_t storage, const void* channel_data, const float* rx_coor
     // Launches of fewer than 2^31 channel samples each, one counter per launch.
     const size_t esz = storage_bytes(storage);
     const int64_t per_tx = static_cast<int64_t>(a.n_rx) * a.row_stride;
-    const int64_t max_tx = std::max<int64_t>(1, ((int64_t{1} << 31) - 1) / std::max<int64_t>(per_tx, 1));
     const int total = a.n_tx;
-    const int64_t n_launch = (std::max(total, 1) + max_tx - 1) / max_tx;
-    if (n_launch > kNoAllocLaunches) {
+    const TransmitSplit split = split_transmits(per_tx, total);
+    if (split.n_launch > kNoAllocLaunches) {
         return fail(MACH_B200_ERR_VALUE,
                     "this job needs %lld launches; the allocation-free call holds work counters for %d (at most "
                     "%d x (2^31 - 1) channel samples)",
-                    static_cast<long long>(n_launch), kNoAllocLaunches, kNoAllocLaunches);
+                    static_cast<long long>(split.n_launch), kNoAllocLaunches, kNoAllocLaunches);
     }
-    MACH_B200_CUDA_TRY(cudaMemsetAsync(counters, 0, sizeof(int) * static_cast<size_t>(n_launch), stream));
+    MACH_B200_CUDA_TRY(cudaMemsetAsync(counters, 0, sizeof(int) * static_cast<size_t>(split.n_launch), stream));
     const char* ch = static_cast<const char*>(a.channel);
     Plan pl = plan;
-    int t0 = 0;
-    for (int64_t launch = 0; launch < n_launch; ++launch) {
+    for (int64_t k = 0; k < split.n_launch; ++k) {
+        const int64_t t0 = launch_first_tx(split, k);
         DasArgs b = a;
-        b.n_tx = static_cast<int32_t>(std::min<int64_t>(max_tx, total - t0));
-        b.channel = ch + static_cast<size_t>(t0) * per_tx * esz;
-        b.arrivals = a.arrivals + static_cast<int64_t>(t0) * a.n_vox;
+        b.n_tx = static_cast<int32_t>(launch_tx_count(split, total, k));
+        b.channel = ch + static_cast<size_t>(t0) * static_cast<size_t>(per_tx) * esz;
+        b.arrivals = a.arrivals + t0 * a.n_vox;
         b.accumulate = t0 == 0 ? a.accumulate : 1;
         CUtensorMap map;
         std::memset(&map, 0, sizeof(map));
@@ -1192,9 +1336,8 @@ int noalloc_impl(int32_t storage, const void* channel_data, const float* rx_coor
                 return rc;
             }
         }
-        pl.ea.counter = counters + launch;
+        pl.ea.counter = counters + k;
         MACH_B200_CUDA_TRY(dispatch(storage, b, interp_type, pl, map, stream));
-        t0 += static_cast<int>(max_tx);
     }
     if (!(flags & MACH_B200_FLAG_ASYNC)) {
         MACH_B200_CUDA_TRY(cudaStreamSynchronize(stream));
@@ -1227,7 +1370,7 @@ struct mach_b200_batch {
 namespace {
 
 struct GroupKey {
-    int family;  // 0 lane-voxel, 1 staged
+    int family;  // 0 lane-voxel, 1 staged, 2 frame-lane
     int storage;
     int interp;
     int variant;  // lane-voxel frame class (1, 0, 16) or staged lanes per voxel
@@ -1241,8 +1384,9 @@ struct GroupKey {
 cudaError_t launch_group(const GroupKey& k, const PersistentLaunch& pl, cudaStream_t st) {
 #define MACH_B200_GCASE(S)                                                                                   \
     case S:                                                                                                   \
-        return k.family == 0 ? launch_lane_voxel_persistent<S>(k.interp, k.variant, k.split != 0, pl, st)     \
-                             : launch_staged_persistent<S>(k.interp, k.variant, pl, st);
+        return k.family == 0   ? launch_lane_voxel_persistent<S>(k.interp, k.variant, k.split != 0, pl, st)   \
+               : k.family == 2 ? launch_frame_lane_persistent<S>(k.interp, k.variant, k.split != 0, pl, st)   \
+                               : launch_staged_persistent<S>(k.interp, k.variant, pl, st);
     g_launches.fetch_add(1, std::memory_order_relaxed);
     switch (k.storage) {
         MACH_B200_GCASE(kF32)
@@ -1253,8 +1397,9 @@ cudaError_t launch_group(const GroupKey& k, const PersistentLaunch& pl, cudaStre
         MACH_B200_GCASE(kCBF16)
         MACH_B200_GCASE(kI16)
         default:
-            return k.family == 0 ? launch_lane_voxel_persistent<kCI16>(k.interp, k.variant, k.split != 0, pl, st)
-                                 : launch_staged_persistent<kCI16>(k.interp, k.variant, pl, st);
+            return k.family == 0   ? launch_lane_voxel_persistent<kCI16>(k.interp, k.variant, k.split != 0, pl, st)
+                   : k.family == 2 ? launch_frame_lane_persistent<kCI16>(k.interp, k.variant, k.split != 0, pl, st)
+                                   : launch_staged_persistent<kCI16>(k.interp, k.variant, pl, st);
     }
 #undef MACH_B200_GCASE
 }
@@ -1344,10 +1489,13 @@ int batch_run(mach_b200_batch* b, const mach_b200_job* jobs, uint32_t n_jobs, cu
         o.tx_chunk = j.tx_chunk;
         o.window_rows = j.window_rows;
         o.lanes_per_voxel = j.lanes_per_voxel;
-        plans[i] = plan_launch(j.storage, j.n_scan, j.n_frames, j.n_tx, j.channel_data, true, o);
+        plans[i] = plan_launch(j.storage, j.n_scan, j.n_frames, j.n_tx, j.channel_data, true, o, j.interp_type, true);
         const Plan& p = plans[i];
         GroupKey k{};
-        if (p.staged) {
+        if (p.frame_lane) {
+            k = {2, j.storage, j.interp_type, p.fl.ring_slots ? p.lp.frame_slots : 104,
+                 (j.flags & MACH_B200_FLAG_SPLIT_DELAY) ? 1 : 0};
+        } else if (p.staged) {
             k = {1, j.storage, j.interp_type, p.lp.lanes_per_voxel, 0};
         } else if (p.lp.kind == kKindLaneVoxel1 || p.lp.kind == kKindLaneVoxelN || p.lp.kind == kKindLaneVoxel16 ||
                    p.lp.kind == kKindLaneVoxel8) {
@@ -1401,6 +1549,8 @@ int batch_run(mach_b200_batch* b, const mach_b200_job* jobs, uint32_t n_jobs, cu
         bj.a.frame_chunks = p.lp.frame_chunks;
         bj.st = p.st;
         bj.st.status = dev->status;
+        bj.fl = p.fl;
+        bj.fl.status = dev->status;
         bj.tiles = static_cast<int32_t>(p.lp.grid.x);
         bj.chunks = static_cast<int32_t>(p.staged ? p.lp.grid.y : 1);
         if (p.staged && p.st.use_tma && bj.a.n_tx > 0) {
@@ -1436,18 +1586,18 @@ int batch_run(mach_b200_batch* b, const mach_b200_job* jobs, uint32_t n_jobs, cu
             b->pending = true;
         }
     }
-    bool any_staged = false;
+    bool any_waits = false;  // staged and frame-lane kernels have bounded waits
     for (int g = 0; g < n_groups; ++g) {
         if (items[g] == 0) continue;
         PersistentLaunch pl{b->d_hdr + g, b->d_jobs + first[g], b->d_begin + first[g], b->d_counters + g, smem[g],
                             max_items[g]};
-        any_staged |= keys[g].family == 1;
+        any_waits |= keys[g].family == 1 || keys[g].family == 2;
         MACH_B200_CUDA_TRY(launch_group(keys[g], pl, stream));
     }
     if (!(flags & MACH_B200_FLAG_ASYNC)) {
         MACH_B200_CUDA_TRY(cudaStreamSynchronize(stream));
         b->pending = false;
-        if (any_staged) return check_status(dev, stream);
+        if (any_waits) return check_status(dev, stream);
     }
     return MACH_B200_OK;
 }
@@ -1570,6 +1720,22 @@ int mach_b200_batch_run(mach_b200_batch* batch, const mach_b200_job* jobs, uint3
 }
 
 void mach_b200_batch_destroy(mach_b200_batch* batch) { batch_free(batch); }
+
+int mach_b200_pool_stats(int32_t device, int32_t reset_high, uint64_t* used_high, uint64_t* reserved) {
+    if (!used_high || !reserved) return fail(MACH_B200_ERR_VALUE, "used_high and reserved must not be NULL");
+    if (device < 0 || device >= kMaxDevices) return fail(MACH_B200_ERR_DEVICE, "device %d out of range", device);
+    *used_high = 0;
+    *reserved = 0;
+    cudaMemPool_t pool = g_devices[device].pool.load();
+    if (pool == nullptr) return MACH_B200_OK;  // nothing allocated on this device yet
+    if (reset_high) {
+        uint64_t zero = 0;
+        MACH_B200_CUDA_TRY(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrUsedMemHigh, &zero));
+    }
+    MACH_B200_CUDA_TRY(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemHigh, used_high));
+    MACH_B200_CUDA_TRY(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, reserved));
+    return MACH_B200_OK;
+}
 
 const char* mach_b200_last_error(void) { return g_error.c_str(); }
 

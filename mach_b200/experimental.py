@@ -52,6 +52,8 @@ def beamform(
     tx_chunk: int = 0,
     delay: str = "auto",
     tile_fast: int = 0,
+    frame_slots: int = 0,
+    prefetch: int = 0,
 ) -> Any:
     """Beamform and coherently compound ``n_transmits`` transmits.
 
@@ -67,8 +69,8 @@ def beamform(
         grid_shape: ``(slow, mid, fast)`` extents when ``scan_coords_m`` is a flattened grid
             (fast = contiguous axis); ``None`` detects it, ``False`` disables tiling by grid.
             Only the voxel-to-CTA assignment depends on it, never the result.
-        kernel, window_rows, lanes_per_voxel, tx_chunk, tile_fast: launch tuning (see
-            ``mach_b200_options`` in include/mach_b200.h); the autotuner sets them.
+        kernel, window_rows, lanes_per_voxel, tx_chunk, tile_fast, frame_slots, prefetch: launch
+            tuning (see ``mach_b200_options`` in include/mach_b200.h); the autotuner sets them.
         delay: ``"reference"`` computes delays in FP32 exactly as mach does (bit-identical
             sample positions); ``"split"`` forms each sample position and phase in FP64 per
             receive path and per transmit as an integer base + FP32 fraction (more accurate,
@@ -85,12 +87,12 @@ def beamform(
                      modulation_freq_hz=modulation_freq_hz, tukey_alpha=tukey_alpha, interp_type=interp_type,
                      channel_scale=channel_scale, sync=sync, grid_shape=grid_shape, kernel=kernel,
                      window_rows=window_rows, lanes_per_voxel=lanes_per_voxel, tx_chunk=tx_chunk, delay=delay,
-                     power=False, tile_fast=tile_fast)
+                     power=False, tile_fast=tile_fast, frame_slots=frame_slots, prefetch=prefetch)
 
 
 def _compound(channel_data, rx_coords_m, scan_coords_m, tx_wave_arrivals_s, out, *, rx_start_s, sampling_freq_hz,
               f_number, sound_speed_m_s, modulation_freq_hz, tukey_alpha, interp_type, channel_scale, sync, grid_shape,
-              kernel, window_rows, lanes_per_voxel, tx_chunk, delay, power, tile_fast=0):
+              kernel, window_rows, lanes_per_voxel, tx_chunk, delay, power, tile_fast=0, frame_slots=0, prefetch=0):
     """Shared body of :func:`beamform` and :func:`mach_b200.doppler.power_doppler` (``power``:
     ``out`` is the float32 ``[n_points]`` power image instead of the frames)."""
     xp = array_namespace(channel_data)
@@ -185,7 +187,7 @@ def _compound(channel_data, rx_coords_m, scan_coords_m, tx_wave_arrivals_s, out,
         grid_shape = _grid.detect(scan_coords_m)
     options = _cuda_impl.make_options(
         flags, grid_shape=grid_shape or None, kernel=kernel, tx_chunk=tx_chunk, window_rows=window_rows,
-        lanes_per_voxel=lanes_per_voxel, tile_fast=tile_fast)
+        lanes_per_voxel=lanes_per_voxel, tile_fast=tile_fast, frame_slots=frame_slots, prefetch=prefetch)
     if waves is not None:
         options.tx_model = waves.model
         options.tx_params = arr.ptr

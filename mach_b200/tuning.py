@@ -2,7 +2,8 @@
 
 The candidates are the launch knobs of ``mach_b200_options`` (include/mach_b200.h):
 kernel family, transmits staged per pass (voxel-per-lane), lanes per voxel and window
-rows (staged windows), and whether to tile by the voxel grid.  None of them changes the
+rows (staged windows), frame columns per warp and L1 prefetch (frame-lane), and whether to
+tile by the voxel grid.  None of them changes the
 result beyond summation order; every candidate is timed with CUDA events on the current
 stream over a few repetitions on the caller's own device-resident data, and the winner
 is cached per job shape and device in a JSON file (``MACH_B200_TUNING_CACHE``, default
@@ -54,6 +55,13 @@ def candidates(storage: str, n_frames: int, grid: Any) -> list[dict]:
                 for g in grids:
                     out.append({"kernel": "staged", "lanes_per_voxel": lv, "window_rows": rows, "grid_shape": g})
     cplx = storage in ("c64", "cf16", "cbf16", "ci16")
+    words = n_frames if cplx else (n_frames // 2 if n_frames % 2 == 0 else 0)
+    if words >= 32:  # lanes = frames, rows reused in registers along runs of 16 / 8 / 4 voxels
+        for slots in (1, 2, 4):
+            if slots > 1 and words <= 32 * (slots // 2):
+                continue
+            for prefetch in (1, 2):
+                out.append({"kernel": "frame_lane", "frame_slots": slots, "prefetch": prefetch})
     if n_frames >= (32 if cplx else 64) and (n_frames * esz) % 16 == 0:
         for rows in (32, 48, 64):
             for g in grids:
@@ -63,8 +71,9 @@ def candidates(storage: str, n_frames: int, grid: Any) -> list[dict]:
     return out
 
 
-def _key(storage, n_tx, n_rx, n_samples, n_frames, n_vox, grid, interp, device_name) -> str:
-    return f"{device_name}|{storage}|tx{n_tx}|rx{n_rx}|s{n_samples}|f{n_frames}|v{n_vox}|g{grid}|i{int(interp)}"
+def _key(storage, n_tx, n_rx, n_samples, n_frames, n_vox, grid, interp, device_name, delay="auto") -> str:
+    return (f"{device_name}|{storage}|tx{n_tx}|rx{n_rx}|s{n_samples}|f{n_frames}|v{n_vox}|g{grid}|i{int(interp)}"
+            f"|d{delay}")
 
 
 def _load() -> dict:
@@ -108,7 +117,7 @@ def tune(channel_data, rx_coords_m, scan_coords_m, tx_wave_arrivals_s, *, reps: 
     n_vox = int(scan_coords_m.shape[0])
     grid = _grid.detect(scan_coords_m)
     key = _key(storage, n_tx, n_rx, n_samples, n_frames, n_vox, grid, params.get("interp_type", 1),
-               torch.cuda.get_device_name(channel_data.device))
+               torch.cuda.get_device_name(channel_data.device), params.get("delay", "auto"))
     if use_cache:
         with _LOCK:
             if key in _MEMO:

@@ -22,7 +22,8 @@ BUILD_DIR = HERE / "_build"
 REF_DIR = HERE / "_ref"
 ORACLE_LIB = BUILD_DIR / "libdas_oracle.so"
 REF_LIB = REF_DIR / "libmachref.so"
-REFERENCE_ROOT = Path(os.environ.get("MACH_REFERENCE_ROOT", "/root/reference"))
+# The mach checkout: MACH_REFERENCE_ROOT, else a checkout named "reference" beside this repository.
+REFERENCE_ROOT = Path(os.environ.get("MACH_REFERENCE_ROOT", HERE.parent.parent / "reference"))
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 

@@ -5,13 +5,27 @@ from mach_b200 import tuning
 
 def test_candidates_cover_the_families():
     kinds = {c["kernel"] for c in tuning.candidates("c64", 64, (1, 256, 256))}
-    assert kinds == {"staged", "ensemble", "warp", "lane_voxel"}
+    assert kinds == {"staged", "ensemble", "warp", "lane_voxel", "frame_lane"}
     kinds = {c["kernel"] for c in tuning.candidates("cf16", 16, None)}
     assert kinds == {"lane_voxel", "staged", "warp"}
     assert {c["kernel"] for c in tuning.candidates("f32", 1, None)} == {"lane_voxel"}
     # long ensembles: 8-frame chunks of the voxel-per-lane kernel next to the ensemble kernel
     kinds = {c["kernel"] for c in tuning.candidates("cf16", 200, (1, 256, 256))}
-    assert {"lane_voxel", "ensemble", "staged", "warp"} <= kinds
+    assert {"lane_voxel", "ensemble", "staged", "warp", "frame_lane"} <= kinds
+
+
+def test_frame_lane_knobs():
+    """Frame columns per warp that leave whole columns empty are not tried; prefetch both ways."""
+    def knobs(storage, n_frames):
+        return {(c["frame_slots"], c["prefetch"]) for c in tuning.candidates(storage, n_frames, (256, 1, 256))
+                if c["kernel"] == "frame_lane"}
+
+    assert knobs("c64", 200) == {(s, p) for s in (1, 2, 4) for p in (1, 2)}
+    assert knobs("c64", 32) == {(1, 1), (1, 2)}
+    assert knobs("c64", 64) == {(s, p) for s in (1, 2) for p in (1, 2)}
+    assert knobs("i16", 128) == {(s, p) for s in (1, 2) for p in (1, 2)}  # 64 lane words of two frames
+    assert knobs("c64", 16) == set()
+    assert knobs("i16", 33) == set()  # odd real frame counts have no lane words of two frames
 
 
 def test_lane_voxel_knobs():

@@ -5,7 +5,10 @@ reserved all of HBM, or a real-time acquisition loop where a memory pool that gr
 call could stall it.  This entry point keeps the kernel's scratch (its work-item counters) in
 a static device array of the library.  The tests call it through the C ABI, twice in a row on
 the same output, and compare each image with mach_b200_beamform_ex (which allocates its
-counters per call) on the same job.
+counters per call) on the same job and with the FP64 oracle.  Around the two calls they check
+that no memory was taken: the high-water marks of the process's default CUDA memory pool and
+of the library's own pool do not move, neither pool reserves more, and torch's allocator holds
+the same bytes.
 
 The file name makes pytest collect it last.
 """
@@ -29,6 +32,54 @@ def _bind():
     fn.argtypes = list(lib.mach_b200_beamform_ex.argtypes)
     fn.restype = ctypes.c_int
     return lib, fn
+
+
+class _MemoryWatch:
+    """High-water marks and reservations of the default pool (CUDA runtime) and of the
+    library's pool (mach_b200_pool_stats), plus torch's allocated bytes."""
+
+    def __init__(self, lib):
+        import torch
+        from cuda.bindings import runtime as rt
+
+        self.lib, self.rt, self.torch = lib, rt, torch
+        self.dev = torch.cuda.current_device()
+        err, self.pool = rt.cudaDeviceGetDefaultMemPool(self.dev)
+        assert err == rt.cudaError_t.cudaSuccess, err
+
+    def _default(self, reset):
+        rt = self.rt
+        if reset:
+            from cuda.bindings import driver
+
+            res = rt.cudaMemPoolSetAttribute(self.pool, rt.cudaMemPoolAttr.cudaMemPoolAttrUsedMemHigh,
+                                             driver.cuuint64_t(0))
+            err = res[0] if isinstance(res, tuple) else res
+            assert err == rt.cudaError_t.cudaSuccess, err
+        err, high = rt.cudaMemPoolGetAttribute(self.pool, rt.cudaMemPoolAttr.cudaMemPoolAttrUsedMemHigh)
+        assert err == rt.cudaError_t.cudaSuccess, err
+        err, reserved = rt.cudaMemPoolGetAttribute(self.pool, rt.cudaMemPoolAttr.cudaMemPoolAttrReservedMemCurrent)
+        assert err == rt.cudaError_t.cudaSuccess, err
+        return int(high), int(reserved)
+
+    def _library(self, reset):
+        high, reserved = ctypes.c_uint64(0), ctypes.c_uint64(0)
+        rc = self.lib.mach_b200_pool_stats(self.dev, int(reset), ctypes.byref(high), ctypes.byref(reserved))
+        assert rc == 0, self.lib.mach_b200_last_error()
+        return high.value, reserved.value
+
+    def start(self):
+        self.torch.cuda.synchronize()
+        self.before = (self._default(True), self._library(True), self.torch.cuda.memory_allocated(),
+                       self.torch.cuda.memory_reserved())
+
+    def check(self):
+        self.torch.cuda.synchronize()
+        (d_high, d_res), (l_high, l_res), t_alloc, t_res = self.before
+        assert self._default(False) == (d_high, d_res), "the default memory pool grew"
+        assert self._library(False) == (l_high, l_res), "the library's memory pool was used"
+        assert self.torch.cuda.memory_allocated() == t_alloc
+        assert self.torch.cuda.memory_reserved() == t_res
 
 
 def _job(storage: str, interp: int = 1):
@@ -70,6 +121,9 @@ def test_noalloc_matches_allocating_entry_point_twice(cuda, storage, interp):
     from mach_b200 import _cuda_impl, _grid
 
     lib, fn = _bind()
+    lib.mach_b200_pool_stats.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(ctypes.c_uint64),
+                                         ctypes.POINTER(ctypes.c_uint64)]
+    lib.mach_b200_pool_stats.restype = ctypes.c_int
     if storage == "i16":  # real RF: a frame pair per lane
         w = H.small("volume3d", n_side=8, n_elem_side=8, n_frames=64)
         ch, scale = w.channel, w.channel_scale
@@ -88,14 +142,21 @@ def test_noalloc_matches_allocating_entry_point_twice(cuda, storage, interp):
     want = torch.zeros(shape, dtype=dtype, device="cuda")
     assert _call(lib.mach_b200_beamform_ex, storage, w, t, p, scale, want, opts) == 0, lib.mach_b200_last_error()
     got = torch.full(shape, 7.0, dtype=dtype, device="cuda")
+    w.params["interp_type"] = interp
+    w.channel_scale = scale
+    oracle = H.oracle(w, channel=t["channel"].cpu(), storage=storage)
+    watch = _MemoryWatch(lib)
     for _ in range(2):  # the second call must find its counters zeroed again
         launches = lib.mach_b200_launch_count()
+        watch.start()
         assert _call(fn, storage, w, t, p, scale, got, opts) == 0, lib.mach_b200_last_error()
+        watch.check()
         assert lib.mach_b200_launch_count() == launches + 1
-        torch.cuda.synchronize()
         a, b = got.cpu().numpy(), want.cpu().numpy()
         assert abs(b).max() > 0
         assert H.rel_l2(a, b) <= 2e-6
+        db = H.nrms_db(a, oracle)
+        assert db <= -60.0, f"{storage}: {db:.1f} dB against the FP64 oracle"
 
 
 def test_noalloc_rejects_what_it_cannot_run(cuda):
