@@ -582,8 +582,26 @@ def _serving_config(args, classes, n):
     }
 
 
+SERVING_SWEEP_HZ = (200.0, 400.0, 600.0, 800.0, 1000.0)
+SERVING_SWEEP_REQUESTS = 300
+
+
+def _serve_once(engine, classes, rate, n, seed):
+    """One stream through an engine; returns (requests, makespan_s, waves, graph replays)."""
+    from mach_b200 import serving
+
+    reqs = serving.poisson_arrivals(rate, n, [c.weight for c in classes], seed=seed)
+    waves0, hits0 = len(engine.scheduler.waves), engine.executor.graph_hits
+    engine.serve(reqs)
+    waves = engine.scheduler.waves[waves0:]
+    return reqs, max(r.done_s for r in reqs), waves, engine.executor.graph_hits - hits0
+
+
 def run_serving(args, world, rank, local):
-    """The serving stream through mach_b200.serving (continuous batching, graph replays)."""
+    """The serving stream through mach_b200.serving (continuous batching, graph replays):
+    `value` with each class's acquisition resident in HBM, `e2e` with every request's own
+    acquisition uploaded from pinned host memory and its image read back, and a rate sweep
+    of the upload mode."""
     from mach_b200 import _cuda_impl, serving
     from mach_b200.batch import Batch, Job
     from oracle import das_fp64, oracle_c
@@ -592,9 +610,8 @@ def run_serving(args, world, rank, local):
     torch.cuda.synchronize()
     torch.cuda.empty_cache()
     engine = serving.ServingEngine(classes, slots_per_class=8)
-    warm = serving.poisson_arrivals(SERVING_RATE_HZ, max(100, args.warmup * SERVING_REQUESTS_PER_STEP),
-                                    [c.weight for c in classes], seed=104)
-    engine.serve(warm)
+    engine.serve(serving.poisson_arrivals(SERVING_RATE_HZ, max(100, args.warmup * SERVING_REQUESTS_PER_STEP),
+                                          [c.weight for c in classes], seed=104))
     reqs = _serving_stream(args, classes)
     barrier(world)
     clocks = ClockSampler(local)
@@ -630,8 +647,7 @@ def run_serving(args, world, rank, local):
                      "traffic": None, "algorithmic_bytes_per_launch": None,
                      "note": "algorithmic bytes of all requests / makespan", "peak_source": peak_kind},
         "clocks": clock_info,
-        "e2e": None,
-        "e2e_note": "serving keeps channel data resident on the device by design (no host copies per request)",
+        "mode": "value: each class's acquisition resident in HBM (output slots only)",
     }
     if rank == 0 and world == 1:
         params = ("f_number", "rx_start_s", "sampling_freq_hz", "sound_speed_m_s", "modulation_freq_hz",
@@ -658,6 +674,39 @@ def run_serving(args, world, rank, local):
             line["cpu_baseline"] = cpu.get("cpu_baseline")
             if line["cpu_baseline"]:
                 line["cpu_baseline"]["sample"] = "plain 2-D class: " + line["cpu_baseline"]["sample"]
+    del engine
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+
+    # ---- upload mode: the same stream, every request's acquisition from pinned host memory
+    if not args.no_e2e:
+        up = serving.ServingEngine(classes, slots_per_class=8, upload=True)
+        _serve_once(up, classes, SERVING_RATE_HZ, max(100, args.warmup * SERVING_REQUESTS_PER_STEP), 104)
+        reqs_u, span_u, waves_u, _ = _serve_once(up, classes, SERVING_RATE_HZ, len(reqs), 4)
+        span_u = max_over_ranks(span_u, world)
+        h2d = sum(up.executor.bytes_per_request(r.cls)[0] for r in reqs_u)
+        d2h = sum(up.executor.bytes_per_request(r.cls)[1] for r in reqs_u)
+        steps = max(1, args.steps)
+        line["e2e"] = {"value": world * sum(classes[r.cls].points for r in reqs_u) / span_u, "unit": "points/s",
+                       "h2d_bytes_per_step": int(h2d / steps), "d2h_bytes_per_step": int(d2h / steps),
+                       "ms_per_step": span_u * 1e3 / steps, "requests_per_s": len(reqs_u) / span_u,
+                       "latency_ms": serving.latency_summary(reqs_u),
+                       "api": "mach_b200.serving upload mode: per-request H2D of its own acquisition from pinned "
+                              "host memory on a copy stream, D2H of its image"}
+        sweep = []
+        for i, rate in enumerate(SERVING_SWEEP_HZ):
+            rq, span, _, _ = _serve_once(up, classes, rate, SERVING_SWEEP_REQUESTS, 200 + i)
+            served = len(rq) / span
+            lat = serving.latency_summary(rq)
+            sweep.append({"rate_hz": rate, "requests_per_s": served, "latency_ms": lat,
+                          "sustained": bool(served >= 0.95 * rate * (1 - 1.0 / len(rq)))})
+        ok = [x for x in sweep if x["sustained"]]
+        line["rate_sweep"] = {"mode": "upload", "requests_per_rate": SERVING_SWEEP_REQUESTS, "points": sweep,
+                              "highest_sustained_hz": max((x["rate_hz"] for x in ok), default=None),
+                              "rule": "sustained: served >= 95% of the offered rate over the stream"}
+        del up
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
     return line
 
 
@@ -676,10 +725,16 @@ def _alone_result(c):
     return out
 
 
+SERVING_REFERENCE_SECONDS = 15.0
+
+
 def run_serving_reference(args, world, rank, local):
-    """mach's kernel served serially: each class's service time (one launch + sync per transmit,
-    float32/complex64 input as mach requires) measured on the GPU, then a FIFO single server
-    over the same arrival stream."""
+    """mach's kernel served serially over the same arrival stream, in real time: each request
+    starts when it has arrived and the previous one is done, and runs mach's path for one job
+    (one launch + cudaDeviceSynchronize per transmit, float32 / complex64 input as mach
+    requires, the request's own acquisition).  `value`: inputs already on the device; `e2e`:
+    host inputs through mach's binding (its CPU staging path) and the image read back.  Each
+    run stops after SERVING_REFERENCE_SECONDS of serving; the requests served by then count."""
     from mach_b200 import serving, workloads as W
     from oracle import machref
 
@@ -688,62 +743,96 @@ def run_serving_reference(args, world, rank, local):
     classes = serving.c4_classes()
     keys = ("f_number", "rx_start_s", "sampling_freq_hz", "sound_speed_m_s", "modulation_freq_hz", "tukey_alpha",
             "interp_type")
-    service = []
-    clocks = ClockSampler(local)
-    clocks.start()
+    prep = []
     for c in classes:
         w = c.workload
         src = "c64" if c.storage in ("cf16", "cbf16", "ci16", "c64") else "f32"
         ch, scale = W.as_storage(w, src)
         ch = (ch * scale).contiguous().cuda() if scale != 1.0 else ch.contiguous().cuda()
-        rx = torch.as_tensor(w.rx_coords_m, device="cuda")
-        scan = torch.as_tensor(w.scan_coords_m, device="cuda")
-        arr = torch.as_tensor(w.tx_wave_arrivals_s, device="cuda")
-        out = torch.zeros((w.n_vox, w.n_frames), dtype=torch.complex64 if ch.is_complex() else torch.float32,
-                          device="cuda")
-        ch_ptrs = [ch[t].data_ptr() for t in range(w.n_tx)]
-        arr_ptrs = [arr[t].data_ptr() for t in range(w.n_tx)]
-        p = {k: w.params[k] for k in keys}
+        acqs = serving.make_acquisitions(ch, 2)  # the two acquisitions our upload mode serves
+        d = {"acq_dev": [a.cuda() for a in acqs], "acq_host": [a.numpy() for a in acqs],
+             "rx": torch.as_tensor(w.rx_coords_m, device="cuda"), "scan": torch.as_tensor(w.scan_coords_m, device="cuda"),
+             "arr": torch.as_tensor(w.tx_wave_arrivals_s, device="cuda"),
+             "rx_h": w.rx_coords_m, "scan_h": w.scan_coords_m, "arr_h": np.ascontiguousarray(w.tx_wave_arrivals_s),
+             "p": {k: w.params[k] for k in keys}, "w": w, "cplx": ch.is_complex()}
+        d["out"] = torch.zeros((w.n_vox, w.n_frames), dtype=torch.complex64 if d["cplx"] else torch.float32,
+                               device="cuda")
+        d["out_h"] = torch.zeros(d["out"].shape, dtype=d["out"].dtype).pin_memory()
+        prep.append(d)
+        del ch
 
-        def step():
-            out.zero_()
-            machref.beamform_device(ch_ptrs, rx.data_ptr(), scan.data_ptr(), arr_ptrs, out.data_ptr(),
-                                    is_complex=ch.is_complex(), n_rx=w.n_rx, n_samples=w.n_samples, n_vox=w.n_vox,
-                                    n_frames=w.n_frames, **p)
-
-        for _ in range(max(1, min(args.warmup, 3))):
-            step()
+    def job(d, acq, host):
+        w = d["w"]
+        d["out"].zero_()
+        if host:
+            machref.beamform_host(d["acq_host"][acq], d["rx_h"], d["scan_h"], d["arr_h"], None,
+                                  out_on_device_ptr=d["out"].data_ptr(), **d["p"])
+            d["out_h"].copy_(d["out"])
+        else:
+            ch, arr = d["acq_dev"][acq], d["arr"]
+            machref.beamform_device([ch[t].data_ptr() for t in range(w.n_tx)], d["rx"].data_ptr(),
+                                    d["scan"].data_ptr(), [arr[t].data_ptr() for t in range(w.n_tx)],
+                                    d["out"].data_ptr(), is_complex=d["cplx"], n_rx=w.n_rx, n_samples=w.n_samples,
+                                    n_vox=w.n_vox, n_frames=w.n_frames, **d["p"])
         torch.cuda.synchronize()
-        times = []
-        for _ in range(5):
-            t0 = time.perf_counter()
-            step()
-            torch.cuda.synchronize()
-            times.append(time.perf_counter() - t0)
-        service.append(float(np.median(times)))
-        del ch, out
-        torch.cuda.empty_cache()
+
+    def serve(host, rate, n, seed, seconds):
+        reqs = serving.poisson_arrivals(rate, n, [c.weight for c in classes], seed=seed)
+        for d in prep:  # warm-up of every class
+            job(d, 0, host)
+        done = []
+        t0 = time.perf_counter()
+        for r in reqs:
+            now = time.perf_counter() - t0
+            if now > seconds:
+                break
+            if now < r.arrival_s:
+                time.sleep(r.arrival_s - now)
+            job(prep[r.cls], r.rid % 2, host)
+            r.done_s = time.perf_counter() - t0
+            done.append(r)
+        return reqs, done, max(r.done_s for r in done)
+
+    clocks = ClockSampler(torch.cuda.current_device())
+    clocks.start()
+    reqs, done, span = serve(False, SERVING_RATE_HZ, max(1, args.steps) * SERVING_REQUESTS_PER_STEP, 4,
+                             SERVING_REFERENCE_SECONDS)
     clock_info = clocks.stop()
-    reqs = _serving_stream(args, classes)
-    done = serving.serial_reference_latencies(reqs, lambda r: service[r.cls])
-    makespan = max(r.done_s for r in done)
     points = sum(classes[r.cls].points for r in done)
-    return {
-        "metric": METRIC, "value": points / makespan, "unit": "points/s", "impl": "reference", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": makespan * 1e3 / max(1, args.steps),
+    line = {
+        "metric": METRIC, "value": points / span, "unit": "points/s", "impl": "reference", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": span * 1e3 / max(1, len(done)) *
+        SERVING_REQUESTS_PER_STEP,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded simulation of the configurations; no public dataset offline)",
-        "config": _serving_config(args, classes, len(reqs)) | {"parallelism": "rank 0 only"},
-        "reference": "mach's kernel (src/mach/kernel.cu, unmodified, sm_100a) called serially per request in arrival "
-                     "order: one launch + cudaDeviceSynchronize per transmit, float32/complex64 input; per-class "
-                     "service time measured on the GPU (median of 5), FIFO single-server queue over the stream",
-        "service_ms": {c.name: s * 1e3 for c, s in zip(classes, service)},
+        "config": _serving_config(args, classes, len(reqs)) | {
+            "parallelism": f"replicas x{world} (one request stream per GPU, no exchange)"},
+        "reference": "mach's kernel (src/mach/kernel.cu, unmodified, sm_100a) serving the same arrival stream serially "
+                     "in real time, one launch + cudaDeviceSynchronize per transmit, float32/complex64 input; rank 0 "
+                     "only",
+        "served_requests": len(done), "served_seconds": span,
         "latency_ms": serving.latency_summary(done),
-        "requests_per_s": len(done) / makespan,
+        "requests_per_s": len(done) / span,
         "clocks": clock_info,
         "gpu_launches": int(sum(classes[r.cls].workload.n_tx for r in done)),
-        "e2e": {"value": points / makespan, "unit": "points/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "mode": "value: each request's acquisition already on the device",
     }
+    if not args.no_e2e:
+        _, done_h, span_h = serve(True, SERVING_RATE_HZ, max(1, args.steps) * SERVING_REQUESTS_PER_STEP, 4,
+                                  SERVING_REFERENCE_SECONDS)
+        # per transmit, mach's binding copies that transmit's channel data and arrivals plus the
+        # element and scan coordinates
+        h2d = sum(prep[r.cls]["acq_host"][0].nbytes + prep[r.cls]["arr_h"].nbytes
+                  + (prep[r.cls]["rx_h"].nbytes + prep[r.cls]["scan_h"].nbytes) * classes[r.cls].workload.n_tx
+                  for r in done_h)
+        d2h = sum(prep[r.cls]["out_h"].numel() * prep[r.cls]["out_h"].element_size() for r in done_h)
+        per_step = len(done_h) / SERVING_REQUESTS_PER_STEP
+        line["e2e"] = {"value": sum(classes[r.cls].points for r in done_h) / span_h, "unit": "points/s",
+                       "h2d_bytes_per_step": int(h2d / per_step), "d2h_bytes_per_step": int(d2h / per_step),
+                       "requests_per_s": len(done_h) / span_h, "served_requests": len(done_h),
+                       "latency_ms": serving.latency_summary(done_h),
+                       "api": "mach's binding with host arrays per transmit (its CPU staging path), image read back"}
+    return line
 
 
 # ----------------------------------------------------------------------------- front end (RF -> IQ, ingest)

@@ -2,20 +2,30 @@
 
 Requests arrive over time (seeded Poisson arrivals) and belong to request classes: a
 beamforming configuration whose geometry (element positions, scan grid, transmit arrival
-times) and acquisitions (channel data) stay resident on the device.  The engine keeps two
-banks of output slots per class; a *wave* is a set of admitted requests that runs as one
-:class:`mach_b200.batch.Batch` (one persistent launch per kernel signature) on its bank's
-stream.  While one wave runs, requests that arrived meanwhile are admitted into the next
-wave on the other bank, so the two waves overlap on the GPU.  A request is admitted when
-its class has a free slot in that bank and the outputs in flight stay within the HBM
-budget (a fraction of the free device memory measured at start-up).  Waves with the same
-slot set are recorded once as a CUDA graph and replayed afterwards.
+times) stays resident on the device.  The engine keeps two banks of slots per class; a
+*wave* is a set of admitted requests that runs as one :class:`mach_b200.batch.Batch` (one
+persistent launch per kernel signature) on its bank's stream.  While one wave runs, requests
+that arrived meanwhile are admitted into the next wave on the other bank, so the two waves
+overlap on the GPU.  A request is admitted when its class has a free slot in that bank and
+the device bytes in flight stay within the HBM budget (a fraction of the free device memory
+measured at start-up).  Waves with the same slot set are recorded once as a CUDA graph and
+replayed afterwards.
+
+Two modes:
+* resident (``upload=False``): every request of a class beamforms the class's acquisition,
+  already on the device; a request holds its output slot (output bytes in flight);
+* upload (``upload=True``): every request carries its own acquisition in pinned host memory.
+  Its channel data is copied into the slot's device input buffer on the bank's copy stream
+  (overlapping the other bank's running wave), beamformed, and its image copied back to a
+  pinned host buffer; a request holds input and output bytes while in flight.
 
 Latency of a request = device completion time of its wave (CUDA event, measured from a
-start event recorded when serving begins) minus its arrival time.
+start event recorded when serving begins; in upload mode after the image is back in host
+memory) minus its arrival time.
 
 mach has no serving layer; its closest equivalent is one synchronous call per transmit of
-each job, in arrival order (``serial_reference_latencies`` models that baseline).
+each job, in arrival order (``serial_reference_latencies`` gives the queue of that baseline
+from measured service times).
 
 The scheduling logic (:class:`Scheduler`) is independent of the GPU: an executor object
 launches waves and reports completions, so the host logic is tested on CPU with a
@@ -43,6 +53,7 @@ class Request:
     done_s: float | None = None  # completion time on the serving clock
     wave: int = -1
     slot: int = -1
+    acq: int = 0  # upload mode: which of the class's acquisitions the request carries
 
 
 def poisson_arrivals(rate_hz: float, n: int, weights: list[float], seed: int) -> list[Request]:
@@ -191,6 +202,7 @@ class RequestClass:
     workload: Any
     storage: str
     tensors: dict = field(default_factory=dict)
+    acquisitions: list = field(default_factory=list)  # upload mode: pinned host channel data
 
     @property
     def points(self) -> int:
@@ -201,7 +213,8 @@ class GpuExecutor:
     """Runs waves as persistent batch launches on one stream per bank; replays CUDA graphs
     for slot sets seen before (``use_graphs``)."""
 
-    def __init__(self, classes: list[RequestClass], slots: list[int], banks: int = 2, use_graphs: bool = True):
+    def __init__(self, classes: list[RequestClass], slots: list[int], banks: int = 2, use_graphs: bool = True,
+                 upload: bool = False, n_acquisitions: int = 2):
         import torch
 
         from mach_b200 import workloads as W
@@ -210,8 +223,11 @@ class GpuExecutor:
         self.torch = torch
         self.classes = classes
         self.use_graphs = use_graphs
+        self.upload = upload
         self.streams = [torch.cuda.Stream() for _ in range(banks)]
+        self.copy_streams = [torch.cuda.Stream() for _ in range(banks)] if upload else []
         self.jobs: list[list[list[Any]]] = []  # [bank][class][slot]
+        self.host_out: list[list[list[Any]]] = []  # upload mode: [bank][class][slot] pinned images
         for c in classes:
             w = c.workload
             ch, scale = W.as_storage(w, c.storage)
@@ -222,18 +238,24 @@ class GpuExecutor:
                 "arr": torch.as_tensor(w.tx_wave_arrivals_s, device="cuda").contiguous(),
                 "scale": scale,
             }
+            if upload:
+                c.acquisitions = make_acquisitions(c.tensors["channel"], n_acquisitions)
         params = ("f_number", "rx_start_s", "sampling_freq_hz", "sound_speed_m_s", "modulation_freq_hz", "tukey_alpha",
                   "interp_type")
         for _ in range(banks):
-            per_class = []
+            per_class, per_class_out = [], []
             for c, n in zip(classes, slots):
                 t = c.tensors
-                per_class.append([
-                    Job(channel=t["channel"], rx_coords_m=t["rx"], scan_coords_m=t["scan"], arrivals=t["arr"],
-                        channel_scale=t["scale"], **{k: c.workload.params[k] for k in params})
-                    for _ in range(n)
-                ])
+                jobs = []
+                for _ in range(n):
+                    channel = torch.empty_like(t["channel"]) if upload else t["channel"]
+                    jobs.append(Job(channel=channel, rx_coords_m=t["rx"], scan_coords_m=t["scan"], arrivals=t["arr"],
+                                    channel_scale=t["scale"], **{k: c.workload.params[k] for k in params}))
+                per_class.append(jobs)
+                if upload:
+                    per_class_out.append([torch.empty(j.out.shape, dtype=j.out.dtype, pin_memory=True) for j in jobs])
             self.jobs.append(per_class)
+            self.host_out.append(per_class_out)
         self.graphs: dict[tuple, Any] = {}
         self.graph_hits = 0
         self.graph_misses = 0
@@ -254,7 +276,18 @@ class GpuExecutor:
         return time.perf_counter() - self.t0
 
     def out_of(self, r: Request, bank: int):
+        """The request's image: the pinned host copy in upload mode, else the device slot."""
+        if self.upload:
+            return self.host_out[bank][r.cls][r.slot]
         return self.jobs[bank][r.cls][r.slot].out
+
+    def bytes_per_request(self, cls: int) -> tuple[int, int]:
+        """(host-to-device, device-to-host) bytes one request of class ``cls`` moves in upload mode."""
+        job = self.jobs[0][cls][0]
+        if not self.upload:
+            return 0, 0
+        ch = job.channel
+        return ch.numel() * ch.element_size(), job.out.numel() * job.out.element_size()
 
     def launch(self, wave: Wave):
         from mach_b200.batch import Batch
@@ -264,6 +297,15 @@ class GpuExecutor:
         order = sorted(wave.requests, key=lambda r: (r.cls, r.slot))
         key = (wave.bank, tuple((r.cls, r.slot) for r in order))
         jobs = [self.jobs[wave.bank][r.cls][r.slot] for r in order]
+        if self.upload:  # each request's acquisition into its slot, on this bank's copy stream
+            copy = self.copy_streams[wave.bank]
+            with torch.cuda.stream(copy):
+                for r, j in zip(order, jobs):
+                    acq = self.classes[r.cls].acquisitions
+                    j.channel.copy_(acq[r.acq % len(acq)], non_blocking=True)
+                uploaded = torch.cuda.Event()
+                uploaded.record(copy)
+            stream.wait_event(uploaded)
         with torch.cuda.stream(stream):
             entry = self.graphs.get(key) if self.use_graphs else None
             if entry is not None:
@@ -282,6 +324,9 @@ class GpuExecutor:
                     batch.capture(warmup=False)
                     self.captured_kernels += batch.kernels
                     self.graphs[key] = batch
+            if self.upload:  # images back to pinned host memory
+                for r, j in zip(order, jobs):
+                    self.host_out[wave.bank][r.cls][r.slot].copy_(j.out, non_blocking=True)
             done = torch.cuda.Event(enable_timing=True)
             done.record(stream)
         return done
@@ -297,25 +342,35 @@ class GpuExecutor:
 
 
 class ServingEngine:
-    """Resident request classes + scheduler + GPU executor."""
+    """Request classes + scheduler + GPU executor (resident or upload mode)."""
 
     def __init__(self, classes: list[RequestClass], *, slots_per_class: int = 8, hbm_fraction: float = 0.5,
-                 max_wave_jobs: int = 32, use_graphs: bool = True, on_done=None):
+                 max_wave_jobs: int = 32, use_graphs: bool = True, on_done=None, upload: bool = False,
+                 n_acquisitions: int = 2):
         import torch
 
         self.classes = classes
-        out_bytes = []
+        self.executor = GpuExecutor(classes, [slots_per_class] * len(classes), use_graphs=use_graphs, upload=upload,
+                                    n_acquisitions=n_acquisitions)
+        # device bytes a request holds in flight: its output, plus its input buffer in upload mode
+        self.bytes_of = []
         for c in classes:
             w = c.workload
             cplx = c.storage in ("c64", "cf16", "cbf16", "ci16")
-            out_bytes.append(w.n_vox * w.n_frames * (8 if cplx else 4))
-        self.executor = GpuExecutor(classes, [slots_per_class] * len(classes), use_graphs=use_graphs)
+            held = w.n_vox * w.n_frames * (8 if cplx else 4)
+            if upload:
+                ch = c.tensors["channel"]
+                held += ch.numel() * ch.element_size()
+            self.bytes_of.append(held)
         free, _total = torch.cuda.mem_get_info()
         self.budget = int(hbm_fraction * free)
-        self.scheduler = Scheduler(self.executor, [slots_per_class] * len(classes), out_bytes, self.budget,
+        self.scheduler = Scheduler(self.executor, [slots_per_class] * len(classes), self.bytes_of, self.budget,
                                    max_wave_jobs=max_wave_jobs, on_done=on_done)
 
     def serve(self, requests: list[Request]) -> list[Request]:
+        for r in requests:  # upload mode: the request's acquisition (the same stream gives the same data)
+            n = max(1, len(self.classes[r.cls].acquisitions))
+            r.acq = r.rid % n
         self.executor.start()
         self.scheduler.serve(requests)
         self.torch_sync()
@@ -326,6 +381,21 @@ class ServingEngine:
         import torch
 
         torch.cuda.synchronize()
+
+
+def make_acquisitions(channel, n: int) -> list:
+    """``n`` distinct acquisitions in pinned host memory with the statistics of ``channel``
+    ([n_tx, n_rx, n_samples, n_frames(, 2)]): the data itself, then copies delayed by 17 k
+    samples (rolled along the sample axis)."""
+    import torch
+
+    out = []
+    for k in range(n):
+        x = channel if k == 0 else torch.roll(channel, shifts=17 * k, dims=2)
+        host = torch.empty(x.shape, dtype=x.dtype, pin_memory=True)
+        host.copy_(x)
+        out.append(host)
+    return out
 
 
 def c4_classes(device: str = "cuda", small: bool = False) -> list[RequestClass]:

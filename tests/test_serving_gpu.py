@@ -58,3 +58,44 @@ def test_results_are_the_same_alone_and_in_the_mix(cuda):
         assert torch.equal(out, alone[r.cls]), (p, rid, classes[r.cls].name)
     lat = serving.latency_summary(reqs)
     assert lat["p50"] > 0
+
+
+def test_uploaded_requests_match_their_acquisition_alone(cuda):
+    """Upload mode: every request carries its own acquisition from pinned host memory (two per
+    class here), uploaded on a copy stream while the other bank's wave runs; its image comes
+    back to pinned host memory and equals, bit for bit, that acquisition beamformed alone."""
+    import torch
+
+    from mach_b200 import serving
+    from mach_b200.batch import Batch, Job
+
+    classes = serving.c4_classes(small=True)
+    results = {}
+
+    def keep(r, wave):
+        results[r.rid] = (r.cls, r.acq, engine.executor.out_of(r, wave.bank).clone())
+
+    engine = serving.ServingEngine(classes, slots_per_class=4, on_done=keep, upload=True, n_acquisitions=2)
+    reqs = serving.poisson_arrivals(20000.0, 48, [c.weight for c in classes], seed=5)
+    engine.serve(reqs)
+    engine.serve(serving.poisson_arrivals(20000.0, 48, [c.weight for c in classes], seed=5))  # graph replays
+    assert engine.executor.graph_hits > 0
+    assert len(results) == 48 and all(not out.is_cuda for _, _, out in results.values())
+    assert {acq for _, acq, _ in results.values()} == {0, 1}
+    # admission counts the input buffer as well as the image
+    assert all(b > c.workload.n_vox * c.workload.n_frames * 4 for b, c in zip(engine.bytes_of, classes))
+    params = ("f_number", "rx_start_s", "sampling_freq_hz", "sound_speed_m_s", "modulation_freq_hz", "tukey_alpha",
+              "interp_type")
+    alone = {}
+    for ci, c in enumerate(classes):
+        t = c.tensors
+        for k, acq in enumerate(c.acquisitions):
+            job = Job(channel=acq.to("cuda"), rx_coords_m=t["rx"], scan_coords_m=t["scan"], arrivals=t["arr"],
+                      channel_scale=t["scale"], **{p: c.workload.params[p] for p in params})
+            b = Batch([job])
+            b.run(sync=True)
+            alone[(ci, k)] = job.out.cpu()
+            b.close()
+        assert not torch.equal(alone[(ci, 0)], alone[(ci, 1)])  # the acquisitions differ
+    for rid, (cls, acq, out) in results.items():
+        assert torch.equal(out, alone[(cls, acq)]), (rid, classes[cls].name, acq)
