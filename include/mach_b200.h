@@ -82,9 +82,9 @@ extern "C" {
 #define MACH_B200_KERNEL_WARP 3       /* a warp per voxel over frames, taps read from global memory */
 #define MACH_B200_KERNEL_ENSEMBLE 4   /* lanes = frames of a 32-lane block, voxel-tile sample windows in
                                          tensor memory (many frames; nearest or linear taps) */
-#define MACH_B200_KERNEL_FRAME_LANE 5 /* lanes = frames, a warp walks a run of neighbouring voxels and
-                                         keeps sample rows in registers (many frames; nearest or
-                                         linear taps) */
+#define MACH_B200_KERNEL_FRAME_LANE 5 /* lanes = frames, a warp walks a run of neighbouring voxels
+                                         and loads each element's sample rows once for all of them
+                                         (many frames; nearest or linear taps) */
 
 /*
  * Optional launch options.  Zero-initialise, set struct_size = sizeof(mach_b200_options),
@@ -116,10 +116,10 @@ typedef struct mach_b200_options {
                                 offset, formed in FP64 and rounded to FP32.  Device or host memory. */
     int32_t frame_slots;     /* frame-lane kernel: columns of 32 lane words (frames) a warp holds, 1, 2
                                 or 4, with runs of 16, 8 or 4 voxels; 0 = automatic */
-    int32_t prefetch;        /* frame-lane kernel: 1 = sample rows loaded straight from global memory;
-                                2 = rows streamed one parameter batch ahead into a shared-memory ring
-                                by bulk copies (needs n_frames x sample bytes a multiple of 16 and a
-                                16-byte aligned channel_data); 0 = automatic (1) */
+    int32_t element_block;   /* voxel-per-lane kernels: elements per launch (the job runs as one launch
+                                per block of elements, accumulating), so that a launch's channel data
+                                stays in L2; 0 = automatic (blocks of about 80 MB of channel data for
+                                16-frame jobs above 126 MB), -1 or >= n_rx = one launch */
 } mach_b200_options;
 
 /* Transmit models (mach_b200_options.tx_model). */

@@ -19,7 +19,7 @@ struct alignas(64) BatchJob {
     CUtensorMap map;  // staged family: TMA view of this job's channel data (64-byte aligned)
     DasArgs a;
     StagedArgs st;
-    FrameLaneArgs fl;  // frame-lane family: run mapping and ring layout
+    FrameLaneArgs fl;  // frame-lane family: run mapping and frame chunks
     int32_t tiles;   // spatial tiles (frame-lane family: CTA blocks)
     int32_t chunks;  // frame chunks per tile (staged family), 1 otherwise
 };
@@ -100,11 +100,11 @@ __global__ void __launch_bounds__(kStagedThreads, 3)
     }
 }
 
-template <int S, int INTERP, int J, bool SPLIT, bool RING>
+template <int S, int INTERP, int J, bool SPLIT>
 __global__ void __launch_bounds__(kFrameLaneThreads, 4)
     das_frame_lane_persistent(const BatchHeader* __restrict__ hdr, const BatchJob* __restrict__ jobs,
                               const int64_t* __restrict__ item_begin, unsigned long long* counter) {
-    extern __shared__ __align__(128) unsigned char smem_raw[];
+    extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ DasArgs s_args;
     __shared__ FrameLaneArgs s_fl;
     __shared__ int s_job;
@@ -114,7 +114,7 @@ __global__ void __launch_bounds__(kFrameLaneThreads, 4)
         copy_words(&s_args, &jobs[s_job].a);
         copy_words(&s_fl, &jobs[s_job].fl);
         __syncthreads();
-        frame_lane_block<S, INTERP, J, 16 / J, SPLIT, RING>(s_args, s_fl, s_local, smem_raw);
+        frame_lane_block<S, INTERP, J, 16 / J, SPLIT>(s_args, s_fl, s_local, smem_raw);
     }
 }
 

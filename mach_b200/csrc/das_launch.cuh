@@ -36,6 +36,8 @@ struct LaunchPlan {
     int map_wlog;
     int64_t map_outer;
     int frame_chunks;   // lane-voxel 8-frame chunks per tile (DasArgs::frame_chunks)
+    int element_block;  // lane-voxel kernels: elements per launch (0 = all), so that one launch's
+                        // channel data stays resident in L2
     int frame_slots;    // frame-lane kernel: J, lane-word columns per warp (1, 2 or 4)
     int run_voxels;     // frame-lane kernel: G, voxels per warp run (J * G = 16)
 };
@@ -123,24 +125,19 @@ cudaError_t launch_das(const DasArgs& a, int interp, const LaunchPlan& p, cudaSt
     return cudaGetLastError();
 }
 
-// Frame-lane kernel: (J, G) pairs with J * G = 16 (64 accumulator registers for complex storage)
-// with the shared-memory row ring; direct row loads with (4, 4).
-template <int S, int I, int J, bool SPLIT, bool RING>
+// Frame-lane kernel: (J, G) pairs with J * G = 16 (64 accumulator registers for complex storage).
+template <int S, int I, int J, bool SPLIT>
 cudaError_t launch_frame_lane_k(const DasArgs& a, const FrameLaneArgs& fl, const LaunchPlan& p, cudaStream_t stream) {
-    auto kernel = das_frame_lane_kernel<S, I, J, 16 / J, SPLIT, RING>;
-    const cudaError_t e = allow_smem(kernel, p.smem);
-    if (e != cudaSuccess) return e;
-    kernel<<<p.grid, p.block, p.smem, stream>>>(a, fl);
+    das_frame_lane_kernel<S, I, J, 16 / J, SPLIT><<<p.grid, p.block, p.smem, stream>>>(a, fl);
     return cudaGetLastError();
 }
 
 template <int S, int I, bool SPLIT>
 cudaError_t launch_frame_lane_i(const DasArgs& a, const FrameLaneArgs& fl, const LaunchPlan& p, cudaStream_t stream) {
-    if (fl.ring_slots == 0) return launch_frame_lane_k<S, I, 4, SPLIT, false>(a, fl, p, stream);
     switch (p.frame_slots) {
-        case 1: return launch_frame_lane_k<S, I, 1, SPLIT, true>(a, fl, p, stream);
-        case 2: return launch_frame_lane_k<S, I, 2, SPLIT, true>(a, fl, p, stream);
-        default: return launch_frame_lane_k<S, I, 4, SPLIT, true>(a, fl, p, stream);
+        case 1: return launch_frame_lane_k<S, I, 1, SPLIT>(a, fl, p, stream);
+        case 2: return launch_frame_lane_k<S, I, 2, SPLIT>(a, fl, p, stream);
+        default: return launch_frame_lane_k<S, I, 4, SPLIT>(a, fl, p, stream);
     }
 }
 
@@ -205,19 +202,18 @@ cudaError_t launch_lane_voxel_persistent(int interp, int frame_class, bool split
 #undef MACH_B200_PLV
 }
 
-// Frame-lane family: variant = J (1, 2, 4) with the row ring, 100 + 4 for direct loads.
+// Frame-lane family: variant = J (1, 2, 4).
 template <int S>
 cudaError_t launch_frame_lane_persistent(int interp, int variant, bool split, const PersistentLaunch& pl,
                                          cudaStream_t stream) {
-#define MACH_B200_PFL(I, J, R)                                                                                      \
-    return split ? launch_persistent(das_frame_lane_persistent<S, I, J, true, R>, kFrameLaneThreads, pl, stream) \
-                 : launch_persistent(das_frame_lane_persistent<S, I, J, false, R>, kFrameLaneThreads, pl, stream)
-#define MACH_B200_PFL_V(I)              \
-    switch (variant) {                  \
-        case 1: MACH_B200_PFL(I, 1, true); \
-        case 2: MACH_B200_PFL(I, 2, true); \
-        case 4: MACH_B200_PFL(I, 4, true); \
-        default: MACH_B200_PFL(I, 4, false); \
+#define MACH_B200_PFL(I, J)                                                                                    \
+    return split ? launch_persistent(das_frame_lane_persistent<S, I, J, true>, kFrameLaneThreads, pl, stream) \
+                 : launch_persistent(das_frame_lane_persistent<S, I, J, false>, kFrameLaneThreads, pl, stream)
+#define MACH_B200_PFL_V(I)           \
+    switch (variant) {               \
+        case 1: MACH_B200_PFL(I, 1); \
+        case 2: MACH_B200_PFL(I, 2); \
+        default: MACH_B200_PFL(I, 4); \
     }
     if (interp == kNearest) {
         MACH_B200_PFL_V(kNearest)

@@ -313,34 +313,9 @@ bool plan_frame_lane(int storage, int interp, uint64_t n_vox, uint32_t n_frames,
     if (words < 32) return false;
     int J = o.frame_slots;
     if (J != 1 && J != 2 && J != 4) J = words <= 32 ? 1 : (words <= 64 ? 2 : 4);
-    // Ring mode (asked for with prefetch = 2; measured slower than direct loads on B200) needs
-    // 16-byte aligned rows for its bulk copies; the direct mode runs (J, G) = (4, 4).
-    const bool ring_ok = o.prefetch == 2 && (words * word_bytes) % 16 == 0 &&
-                         (!channel_on_device || reinterpret_cast<uintptr_t>(channel) % 16 == 0);
-    const int coef = cplx ? 2 : 1;
-    int slots = 0;
-    if (ring_ok) {
-        // Row buffers per warp: the most (a power of two, 4..16) that keep a CTA of four warps
-        // within 56 KB, so that four CTAs fit an SM.
-        const int slot_bytes = 32 * J * word_bytes;
-        for (int k = 16; k >= 4; k >>= 1) {
-            const int wb = coef == 2 ? frame_lane_warp_bytes<2>(k, slot_bytes) : frame_lane_warp_bytes<1>(k, slot_bytes);
-            if (kFrameLaneWarps * wb <= 56 * 1024) {
-                slots = k;
-                break;
-            }
-        }
-    }
-    if (slots == 0) {
-        J = 4;
-    }
     const int G = 16 / J;
+    const int coef = cplx ? 2 : 1;
     FrameLaneArgs& fl = p.fl;
-    fl.slot_bytes = 32 * J * word_bytes;
-    fl.ring_slots = slots;
-    fl.ring_log2 = slots == 16 ? 4 : (slots == 8 ? 3 : (slots == 4 ? 2 : 0));
-    fl.warp_bytes = coef == 2 ? frame_lane_warp_bytes<2>(slots, fl.slot_bytes)
-                              : frame_lane_warp_bytes<1>(slots, fl.slot_bytes);
     if (grid_matches(o, n_vox)) {
         const int64_t slow = o.grid_shape[0], mid = o.grid_shape[1], fast = o.grid_shape[2];
         fl.n_fast = fast;
@@ -376,14 +351,16 @@ bool plan_frame_lane(int storage, int interp, uint64_t n_vox, uint32_t n_frames,
     p.lp.passes = 1;
     p.lp.tx_chunk = 1;
     p.lp.lanes_per_voxel = 32;
-    p.lp.smem = static_cast<size_t>(kFrameLaneWarps) * fl.warp_bytes;
+    p.lp.smem = static_cast<size_t>(kFrameLaneWarps) *
+                (coef == 2 ? frame_lane_warp_bytes<2>() : frame_lane_warp_bytes<1>());
     return true;
 }
 
 // interp < 0: a caller that runs neither the frame-lane nor the ensemble kernel; batch: a
 // persistent batch, which runs the frame-lane kernel but not the ensemble kernel.
 Plan plan_launch(int storage, uint64_t n_vox, uint32_t n_frames, uint32_t n_tx, const void* channel,
-                 bool channel_on_device, const mach_b200_options& o, int interp = -1, bool batch = false) {
+                 bool channel_on_device, const mach_b200_options& o, int interp = -1, bool batch = false,
+                 uint32_t n_rx = 0, uint32_t n_samples = 0) {
     Plan p;
     const int esz = static_cast<int>(storage_bytes(storage));
     const int vf = 8 / esz;
@@ -397,7 +374,10 @@ Plan plan_launch(int storage, uint64_t n_vox, uint32_t n_frames, uint32_t n_tx, 
     // Measured on B200 (200-frame Doppler): for 4-byte complex storage (cf16, cbf16, ci16) the
     // 8-frame chunks beat the ensemble kernel (3.5 vs 5.5 ms); for complex64 and real storage
     // the ensemble kernel wins.
-    if (kind == MACH_B200_KERNEL_AUTO && lane8_ok && esz == 4 && (storage & 1) && grid_matches(o, n_vox)) {
+    // Measured on B200 (200-frame Doppler): the 8-frame chunks beat the ensemble kernel for
+    // complex storage -- 3.3 vs 5.6 ms (cf16), 4.0 vs 4.8 ms (complex64, 256-bit row loads).
+    if (kind == MACH_B200_KERNEL_AUTO && lane8_ok && (esz == 4 || esz == 8) && (storage & 1) &&
+        grid_matches(o, n_vox)) {
         kind = MACH_B200_KERNEL_LANE_VOXEL;
     }
     // Frame-lane kernel: when asked for (measured on B200, the ensemble kernel and the 8-frame
@@ -469,6 +449,19 @@ Plan plan_launch(int storage, uint64_t n_vox, uint32_t n_frames, uint32_t n_tx, 
         if (p.lp.kind == kKindLaneVoxel8) {  // the 8-frame chunks of a tile run on consecutive CTAs
             p.lp.frame_chunks = static_cast<int>(n_frames / 8);
             p.lp.grid.x *= static_cast<unsigned>(p.lp.frame_chunks);
+        }
+        // Element blocks: one launch per block of elements whose channel data (all transmits)
+        // fits in L2 with room to spare.  Automatic for 16-frame jobs above 126 MB of channel
+        // data (3-D: every CTA sweeps every (transmit, element) row set, and CTAs that drift apart
+        // evict each other's rows; measured DRAM reads were 70x the channel data in one launch).
+        {
+            const uint64_t per_elem = static_cast<uint64_t>(n_tx) * n_samples * n_frames * esz;
+            int eb = o.element_block;
+            if (eb == 0 && n_frames == 16 && per_elem > 0 &&
+                per_elem * n_rx > (uint64_t{126} << 20) && !batch) {
+                eb = static_cast<int>(std::max<uint64_t>(32, ((uint64_t{80} << 20) / per_elem) / 32 * 32));
+            }
+            p.lp.element_block = eb > 0 ? eb : 0;
         }
         // split mode stages three words per (transmit, voxel): base, fraction, phase cycles
         p.lp.smem = static_cast<size_t>(p.lp.tx_chunk) * kLaneVoxelThreads * sizeof(float) *
@@ -636,13 +629,21 @@ int dispatch_split(int storage, DasArgs a, int interp, const Plan& plan, cudaStr
         MACH_B200_CUDA_TRY(counters.alloc(sizeof(int) * static_cast<size_t>(split.n_launch), st));
         MACH_B200_CUDA_TRY(cudaMemsetAsync(counters.ptr, 0, sizeof(int) * static_cast<size_t>(split.n_launch), st));
     }
+    // Lane-voxel kernels may run the elements in blocks, one launch each, so that a launch's
+    // channel data stays in L2 while every CTA sweeps it.
+    const bool lane_voxel = !plan.staged && !plan.ensemble && !plan.frame_lane &&
+                            (plan.lp.kind == kKindLaneVoxel1 || plan.lp.kind == kKindLaneVoxelN ||
+                             plan.lp.kind == kKindLaneVoxel16 || plan.lp.kind == kKindLaneVoxel8);
+    const int eblk = lane_voxel && plan.lp.element_block > 0 ? plan.lp.element_block : std::max(a.n_rx, 1);
     for (int64_t k = 0; k < split.n_launch; ++k) {
         const int64_t t0 = launch_first_tx(split, k);
         DasArgs b = a;
         b.n_tx = static_cast<int32_t>(launch_tx_count(split, total, k));
         b.channel = ch + static_cast<size_t>(t0) * static_cast<size_t>(per_tx) * esz;
         b.arrivals = a.arrivals + t0 * a.n_vox;
-        b.accumulate = t0 == 0 ? a.accumulate : 1;
+        b.row32 = (reinterpret_cast<uintptr_t>(b.channel) % 32 == 0 && (static_cast<size_t>(a.n_frames) * esz) % 32 == 0)
+                      ? 1
+                      : 0;
         CUtensorMap map;
         std::memset(&map, 0, sizeof(map));
         if ((plan.staged || plan.ensemble) && plan.st.use_tma && b.n_tx > 0) {
@@ -653,7 +654,14 @@ int dispatch_split(int storage, DasArgs a, int interp, const Plan& plan, cudaStr
             if (rc) return rc;
         }
         if (plan.ensemble) pl.ea.counter = static_cast<int*>(counters.ptr) + k;
-        MACH_B200_CUDA_TRY(dispatch(storage, b, interp, pl, map, st));
+        int e0 = 0;
+        do {
+            b.e_begin = e0;
+            b.e_end = std::min(a.n_rx, e0 + eblk);
+            b.accumulate = (t0 == 0 && e0 == 0) ? a.accumulate : 1;
+            MACH_B200_CUDA_TRY(dispatch(storage, b, interp, pl, map, st));
+            e0 += eblk;
+        } while (e0 < a.n_rx);
     }
     return MACH_B200_OK;
 }
@@ -705,6 +713,8 @@ DasArgs make_args(const float* rx_coords_m, const float* scan_coords_m, uint64_t
     a.scan = scan_coords_m;
     a.n_vox = static_cast<int64_t>(n_scan);
     a.n_rx = static_cast<int32_t>(n_rx);
+    a.e_begin = 0;
+    a.e_end = a.n_rx;
     a.n_samples = static_cast<int32_t>(n_samples);
     a.n_frames = static_cast<int32_t>(n_frames);
     a.row_stride = static_cast<int64_t>(n_samples) * n_frames;
@@ -810,9 +820,9 @@ int compound_impl(int32_t storage, const void* channel_data, const float* rx_coo
                           rx_start_s, sampling_freq_hz, sound_speed_m_s, modulation_freq_hz, tukey_alpha,
                           channel_scale, cplx, flags);
     const bool overwrite = (flags & MACH_B200_FLAG_OVERWRITE) != 0u || r_out != kOnDevice;
-    Plan plan = plan_launch(storage, n_scan, n_frames, n_tx, channel_data, r_ch == kOnDevice, opt, interp_type);
+    Plan plan = plan_launch(storage, n_scan, n_frames, n_tx, channel_data, r_ch == kOnDevice, opt, interp_type, false,
+                            n_rx, n_samples);
     plan.st.status = dev->status;
-    plan.fl.status = dev->status;
     a.frame_passes = plan.lp.passes;
     a.tx_chunk = plan.lp.tx_chunk;
     a.map_fast = plan.lp.map_fast;
@@ -831,7 +841,7 @@ int compound_impl(int32_t storage, const void* channel_data, const float* rx_coo
         if ((rc = dispatch_split(storage, a, interp_type, plan, stream))) return rc;
         if (!(flags & MACH_B200_FLAG_ASYNC)) {
             MACH_B200_CUDA_TRY(cudaStreamSynchronize(stream));
-            if (plan.staged || plan.ensemble || plan.frame_lane) return check_status(dev, stream);
+            if (plan.staged || plan.ensemble) return check_status(dev, stream);
         }
         return MACH_B200_OK;
     }
@@ -924,7 +934,7 @@ int compound_impl(int32_t storage, const void* channel_data, const float* rx_coo
     }
     // Host buffers are in use until the stream drains: always synchronous here.
     MACH_B200_CUDA_TRY(cudaStreamSynchronize(stream));
-    if (plan.staged || plan.ensemble || plan.frame_lane) return check_status(dev, stream);
+    if (plan.staged || plan.ensemble) return check_status(dev, stream);
     return MACH_B200_OK;
 }
 
@@ -1033,7 +1043,6 @@ int power_impl(int32_t storage, const void* channel_data, const float* rx_coords
         const int64_t per_tx = static_cast<int64_t>(n_rx) * n_samples * n_frames;
         if ((plan.ensemble || plan.frame_lane) && per_tx * n_tx < (int64_t{1} << 31)) {
             plan.st.status = dev->status;
-            plan.fl.status = dev->status;
             DasArgs a = make_args(rx_coords_m, scan_coords_m, n_scan, n_rx, n_samples, n_frames, f_number, rx_start_s,
                                   sampling_freq_hz, sound_speed_m_s, modulation_freq_hz, tukey_alpha, channel_scale,
                                   cplx, flags);
@@ -1493,8 +1502,7 @@ int batch_run(mach_b200_batch* b, const mach_b200_job* jobs, uint32_t n_jobs, cu
         const Plan& p = plans[i];
         GroupKey k{};
         if (p.frame_lane) {
-            k = {2, j.storage, j.interp_type, p.fl.ring_slots ? p.lp.frame_slots : 104,
-                 (j.flags & MACH_B200_FLAG_SPLIT_DELAY) ? 1 : 0};
+            k = {2, j.storage, j.interp_type, p.lp.frame_slots, (j.flags & MACH_B200_FLAG_SPLIT_DELAY) ? 1 : 0};
         } else if (p.staged) {
             k = {1, j.storage, j.interp_type, p.lp.lanes_per_voxel, 0};
         } else if (p.lp.kind == kKindLaneVoxel1 || p.lp.kind == kKindLaneVoxelN || p.lp.kind == kKindLaneVoxel16 ||
@@ -1536,6 +1544,10 @@ int batch_run(mach_b200_batch* b, const mach_b200_job* jobs, uint32_t n_jobs, cu
                          j.f_number, j.rx_start_s, j.sampling_freq_hz, j.sound_speed_m_s, j.modulation_freq_hz,
                          j.tukey_alpha, j.channel_scale, cplx, j.flags);
         bj.a.channel = j.channel_data;
+        bj.a.row32 = (reinterpret_cast<uintptr_t>(j.channel_data) % 32 == 0 &&
+                      (static_cast<size_t>(j.n_frames) * storage_bytes(j.storage)) % 32 == 0)
+                         ? 1
+                         : 0;
         bj.a.arrivals = j.tx_wave_arrivals_s;
         bj.a.out = j.out;
         bj.a.n_tx = static_cast<int32_t>(need_channel ? j.n_tx : 0);
@@ -1550,7 +1562,6 @@ int batch_run(mach_b200_batch* b, const mach_b200_job* jobs, uint32_t n_jobs, cu
         bj.st = p.st;
         bj.st.status = dev->status;
         bj.fl = p.fl;
-        bj.fl.status = dev->status;
         bj.tiles = static_cast<int32_t>(p.lp.grid.x);
         bj.chunks = static_cast<int32_t>(p.staged ? p.lp.grid.y : 1);
         if (p.staged && p.st.use_tma && bj.a.n_tx > 0) {
@@ -1586,12 +1597,12 @@ int batch_run(mach_b200_batch* b, const mach_b200_job* jobs, uint32_t n_jobs, cu
             b->pending = true;
         }
     }
-    bool any_waits = false;  // staged and frame-lane kernels have bounded waits
+    bool any_waits = false;  // staged kernels have bounded waits
     for (int g = 0; g < n_groups; ++g) {
         if (items[g] == 0) continue;
         PersistentLaunch pl{b->d_hdr + g, b->d_jobs + first[g], b->d_begin + first[g], b->d_counters + g, smem[g],
                             max_items[g]};
-        any_waits |= keys[g].family == 1 || keys[g].family == 2;
+        any_waits |= keys[g].family == 1;
         MACH_B200_CUDA_TRY(launch_group(keys[g], pl, stream));
     }
     if (!(flags & MACH_B200_FLAG_ASYNC)) {

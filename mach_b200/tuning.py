@@ -2,8 +2,8 @@
 
 The candidates are the launch knobs of ``mach_b200_options`` (include/mach_b200.h):
 kernel family, transmits staged per pass (voxel-per-lane), lanes per voxel and window
-rows (staged windows), frame columns per warp and L1 prefetch (frame-lane), and whether to
-tile by the voxel grid.  None of them changes the
+rows (staged windows), frame columns per warp (frame-lane), and whether to tile by the voxel
+grid.  None of them changes the
 result beyond summation order; every candidate is timed with CUDA events on the current
 stream over a few repetitions on the caller's own device-resident data, and the winner
 is cached per job shape and device in a JSON file (``MACH_B200_TUNING_CACHE``, default
@@ -45,6 +45,9 @@ def candidates(storage: str, n_frames: int, grid: Any) -> list[dict]:
                 for lanes in ((1, 4) if n_frames == 1 else (0,)):
                     out.append({"kernel": "lane_voxel", "tx_chunk": tx_chunk, "tile_fast": tile_fast,
                                 "lanes_per_voxel": lanes})
+    if n_frames == 16:  # elements per launch (L2-resident channel data per launch)
+        for block in (-1, 64, 128, 256):
+            out.append({"kernel": "lane_voxel", "element_block": block})
     if n_frames % vf == 0 and n_frames > 1:
         lv_max = 32 if storage in ("f32", "c64") else 16
         needed = -(-n_frames // vf)
@@ -56,12 +59,11 @@ def candidates(storage: str, n_frames: int, grid: Any) -> list[dict]:
                     out.append({"kernel": "staged", "lanes_per_voxel": lv, "window_rows": rows, "grid_shape": g})
     cplx = storage in ("c64", "cf16", "cbf16", "ci16")
     words = n_frames if cplx else (n_frames // 2 if n_frames % 2 == 0 else 0)
-    if words >= 32:  # lanes = frames, rows reused in registers along runs of 16 / 8 / 4 voxels
+    if words >= 32:  # lanes = frames, each element's rows loaded once for runs of 16 / 8 / 4 voxels
         for slots in (1, 2, 4):
             if slots > 1 and words <= 32 * (slots // 2):
                 continue
-            for prefetch in (1, 2):
-                out.append({"kernel": "frame_lane", "frame_slots": slots, "prefetch": prefetch})
+            out.append({"kernel": "frame_lane", "frame_slots": slots})
     if n_frames >= (32 if cplx else 64) and (n_frames * esz) % 16 == 0:
         for rows in (32, 48, 64):
             for g in grids:

@@ -1,6 +1,6 @@
 """The frame-lane kernel (lanes = frames, sample rows kept in registers along voxel runs)
 computes the same sums as the other kernel families for every storage type, tap kind, frame
-count, run length, prefetch setting and tiling, matches mach's kernel and the FP64 oracle,
+count, run length, row span and tiling, matches mach's kernel and the FP64 oracle,
 accumulates into a GPU `out`, and fuses the power-Doppler epilogue."""
 
 from __future__ import annotations
@@ -44,14 +44,20 @@ def test_frame_lane_real_frame_pairs(cuda, n_frames):
     assert H.rel_l2(_run(w, kernel="frame_lane"), _run(w, kernel="warp")) <= 2e-6
 
 
-@pytest.mark.parametrize("prefetch", [1, 2])
 @pytest.mark.parametrize("grid", [None, False])
-def test_frame_lane_prefetch_and_tiling(cuda, prefetch, grid):
-    """Runs along the grid's lateral axis or of consecutive voxels; prefetch on or off."""
+def test_frame_lane_tiling(cuda, grid):
+    """Runs along the grid's lateral axis, or of consecutive voxels without a grid."""
     w = _workload("cf16", 64, 1)
     base = _run(w, kernel="warp")
-    got = _run(w, kernel="frame_lane", prefetch=prefetch, grid_shape=grid)
+    got = _run(w, kernel="frame_lane", grid_shape=grid)
     assert H.rel_l2(got, base) <= 2e-6
+
+
+def test_frame_lane_wide_row_spans(cuda):
+    """A coarse lateral grid: the rows of one element's voxels span more than the four held at
+    once, so points load their rows one voxel at a time."""
+    w = H.small("doppler", n_x=9, n_z=16, n_tx=2, n_frames=64, n_elements=40)  # 4 mm lateral steps
+    assert H.rel_l2(_run(w, kernel="frame_lane"), _run(w, kernel="warp")) <= 2e-6
 
 
 def test_frame_lane_ragged_grid(cuda):
@@ -79,12 +85,6 @@ def test_frame_lane_matches_reference_kernel(cuda):
     got = _run(w, kernel="frame_lane", delay="reference")
     ref = H.reference_compound(w)
     assert H.rel_l2(got, ref) <= 1e-5
-
-
-def test_frame_lane_default_is_direct_loads(cuda):
-    """Without a prefetch option the kernel loads rows straight from global memory."""
-    w = _workload("c64", 64, 1)
-    assert np.array_equal(_run(w, kernel="frame_lane"), _run(w, kernel="frame_lane", prefetch=1))
 
 
 def test_frame_lane_accumulates_into_gpu_out(cuda):

@@ -174,3 +174,15 @@ def test_lane_voxel_frame_chunks(cuda, storage, n_frames):
     assert H.nrms_db(chunks, H.oracle(w, storage=storage)) <= -60.0
     if storage in ("cf16", "cbf16", "ci16"):
         np.testing.assert_array_equal(_run(w), chunks)  # the automatic choice
+
+
+@pytest.mark.parametrize("block", [32, 64, -1])
+def test_lane_voxel_element_blocks(cuda, block):
+    """A job run as one launch per block of elements (accumulating) gives the one-launch sums
+    to FP32 rounding, and the oracle's."""
+    w = H.small("volume3d", n_side=8, n_elem_side=12, n_frames=16, n_samples=1400)  # 144 elements
+    one = _run(w, kernel="lane_voxel", element_block=-1)
+    got = _run(w, kernel="lane_voxel", element_block=block)
+    assert np.abs(one).max() > 0
+    assert H.rel_l2(got, one) <= 1e-6
+    assert H.nrms_db(got, H.oracle(w)) <= -60.0

@@ -15,15 +15,15 @@ def test_candidates_cover_the_families():
 
 
 def test_frame_lane_knobs():
-    """Frame columns per warp that leave whole columns empty are not tried; prefetch both ways."""
+    """Frame columns per warp that would leave whole columns empty are not tried."""
     def knobs(storage, n_frames):
-        return {(c["frame_slots"], c["prefetch"]) for c in tuning.candidates(storage, n_frames, (256, 1, 256))
+        return {c["frame_slots"] for c in tuning.candidates(storage, n_frames, (256, 1, 256))
                 if c["kernel"] == "frame_lane"}
 
-    assert knobs("c64", 200) == {(s, p) for s in (1, 2, 4) for p in (1, 2)}
-    assert knobs("c64", 32) == {(1, 1), (1, 2)}
-    assert knobs("c64", 64) == {(s, p) for s in (1, 2) for p in (1, 2)}
-    assert knobs("i16", 128) == {(s, p) for s in (1, 2) for p in (1, 2)}  # 64 lane words of two frames
+    assert knobs("c64", 200) == {1, 2, 4}
+    assert knobs("c64", 32) == {1}
+    assert knobs("c64", 64) == {1, 2}
+    assert knobs("i16", 128) == {1, 2}  # 64 lane words of two frames
     assert knobs("c64", 16) == set()
     assert knobs("i16", 33) == set()  # odd real frame counts have no lane words of two frames
 
