@@ -85,7 +85,8 @@ def parse_args():
     p.add_argument("--also", default=None,
                    help="extra workload:storage lines measured in the same run (default with the default "
                         "workload: doppler:c64,doppler:cf16; 'none' for none)")
-    p.add_argument("--tune", action="store_true", help="run the autotuner on the job during warm-up")
+    p.add_argument("--no-tune", dest="tune", action="store_false",
+                   help="skip the autotuner pass in warm-up (run the planner's automatic choice)")
     p.add_argument("--launch", default="",
                    help="launch options for the headline job, e.g. kernel=frame_lane,frame_slots=4 (profiling)")
     return p.parse_args()
@@ -364,7 +365,7 @@ def measure_ours(args, name, storage, world, rank, local, headline):
         for item in args.launch.split(","):
             key, _, val = item.partition("=")
             knobs[key.strip()] = val.strip() if key.strip() == "kernel" else int(val)
-    if args.tune:
+    if args.tune and not knobs:
         from mach_b200 import tuning
 
         knobs = tuning.tune(ch, rx, scan, arr, channel_scale=w.storage_scale, delay=delay_mode(storage), **p)
@@ -426,13 +427,13 @@ def measure_ours(args, name, storage, world, rank, local, headline):
         "gpu_launches": int(launches),
         "launch": {"delay": delay,
                    "grid_shape": list(grid_shape) if grid_shape else None, "knobs": knobs or None,
-                   "tuned": bool(args.tune)},
+                   "tuned": bool(args.tune and not (headline and args.launch))},
     }
     kernel_s = statistics.mean(per_step) / 1e3
     line["roofline"] = roofline(w, storage, kernel_s, f"{name}:{storage}")
     line["clocks"] = clock_info
     if not args.no_e2e:
-        line["e2e"] = run_e2e(args, w, storage, ch, world, local, knobs)
+        line["e2e"] = run_e2e(args, w, storage, ch, world, local, dict(knobs, grid_shape=grid_shape or False))
     if rank == 0 and world == 1:
         line.update(accuracy_and_baselines(args, w, storage, result, cpu_baseline=headline))
     del ch, rx, scan, arr, out, result, v_ch, v_out
@@ -607,6 +608,15 @@ def run_serving(args, world, rank, local):
     from oracle import das_fp64, oracle_c
 
     classes = serving.c4_classes()
+    if args.tune:  # one autotuner pass per class; the engine's batch jobs run the tuned knobs
+        from mach_b200 import tuning, workloads as W
+
+        for c in classes:
+            w = c.workload
+            ch, scale = W.as_storage(w, c.storage)
+            tuning.tune(ch.contiguous().cuda(), torch.as_tensor(w.rx_coords_m, device="cuda"),
+                        torch.as_tensor(w.scan_coords_m, device="cuda"),
+                        torch.as_tensor(w.tx_wave_arrivals_s, device="cuda"), channel_scale=scale, **w.params)
     torch.cuda.synchronize()
     torch.cuda.empty_cache()
     engine = serving.ServingEngine(classes, slots_per_class=8)
@@ -640,6 +650,7 @@ def run_serving(args, world, rank, local):
             "parallelism": f"replicas x{world} (one request stream per GPU, no exchange)"},
         "latency_ms": serving.latency_summary(reqs),
         "requests_per_s": len(reqs) / makespan,
+        "tuned": {c.name: serving.class_tuning(c) for c in classes} if args.tune else None,
         "waves": {"count": len(waves), "mean_requests": float(np.mean([len(w.requests) for w in waves])),
                   "graph_replays": engine.executor.graph_hits - hits0},
         "gpu_launches": int(launches),

@@ -91,6 +91,20 @@ def beamform(
                      element_block=element_block)
 
 
+def _tuned(storage, n_tx, n_rx, n_samples, n_frames, n_points, grid, interp_type, delay, channel_data):
+    """Cached autotuner knobs for this job on the channel data's (or the current) CUDA device."""
+    from mach_b200 import tuning
+
+    index = 0
+    if _dlpack.is_torch(channel_data) and channel_data.device.type == "cuda":
+        index = channel_data.device.index or 0
+    else:
+        import torch
+
+        index = torch.cuda.current_device()
+    return tuning.lookup(storage, n_tx, n_rx, n_samples, n_frames, n_points, grid, int(interp_type), index, delay)
+
+
 def _compound(channel_data, rx_coords_m, scan_coords_m, tx_wave_arrivals_s, out, *, rx_start_s, sampling_freq_hz,
               f_number, sound_speed_m_s, modulation_freq_hz, tukey_alpha, interp_type, channel_scale, sync, grid_shape,
               kernel, window_rows, lanes_per_voxel, tx_chunk, delay, power, tile_fast=0, frame_slots=0, element_block=0):
@@ -186,6 +200,20 @@ def _compound(channel_data, rx_coords_m, scan_coords_m, tx_wave_arrivals_s, out,
         flags |= _cuda_impl.FLAG_POWER_DOPPLER
     if grid_shape is None:
         grid_shape = _grid.detect(scan_coords_m)
+        if (kernel == "auto" and not (window_rows or lanes_per_voxel or tx_chunk or tile_fast or frame_slots
+                                      or element_block) and not power):
+            # launch knobs the autotuner chose for this job shape, if it has timed one
+            tuned = _tuned(storage, n_tx, n_rx, n_samples, n_frames, n_points, grid_shape, interp_type, delay,
+                           channel_data)
+            if tuned:
+                grid_shape = tuned.pop("grid_shape", grid_shape)
+                kernel = tuned.get("kernel", kernel)
+                window_rows = tuned.get("window_rows", 0)
+                lanes_per_voxel = tuned.get("lanes_per_voxel", 0)
+                tx_chunk = tuned.get("tx_chunk", 0)
+                tile_fast = tuned.get("tile_fast", 0)
+                frame_slots = tuned.get("frame_slots", 0)
+                element_block = tuned.get("element_block", 0)
     options = _cuda_impl.make_options(
         flags, grid_shape=grid_shape or None, kernel=kernel, tx_chunk=tx_chunk, window_rows=window_rows,
         lanes_per_voxel=lanes_per_voxel, tile_fast=tile_fast, frame_slots=frame_slots, element_block=element_block)

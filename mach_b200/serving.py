@@ -242,15 +242,17 @@ class GpuExecutor:
                 c.acquisitions = make_acquisitions(c.tensors["channel"], n_acquisitions)
         params = ("f_number", "rx_start_s", "sampling_freq_hz", "sound_speed_m_s", "modulation_freq_hz", "tukey_alpha",
                   "interp_type")
+        knobs = [class_tuning(c) for c in classes]
         for _ in range(banks):
             per_class, per_class_out = [], []
-            for c, n in zip(classes, slots):
+            for c, n, tuned in zip(classes, slots, knobs):
                 t = c.tensors
                 jobs = []
                 for _ in range(n):
                     channel = torch.empty_like(t["channel"]) if upload else t["channel"]
                     jobs.append(Job(channel=channel, rx_coords_m=t["rx"], scan_coords_m=t["scan"], arrivals=t["arr"],
-                                    channel_scale=t["scale"], **{k: c.workload.params[k] for k in params}))
+                                    channel_scale=t["scale"], tuning=dict(tuned),
+                                    **{k: c.workload.params[k] for k in params}))
                 per_class.append(jobs)
                 if upload:
                     per_class_out.append([torch.empty(j.out.shape, dtype=j.out.dtype, pin_memory=True) for j in jobs])
@@ -381,6 +383,19 @@ class ServingEngine:
         import torch
 
         torch.cuda.synchronize()
+
+
+def class_tuning(c: RequestClass) -> dict:
+    """Autotuner knobs cached for the class's job shape (empty when it has not been timed)."""
+    import torch
+
+    from mach_b200 import _grid, tuning
+
+    ch = c.tensors["channel"]
+    n_tx, n_rx, n_s, n_f = (int(d) for d in ch.shape[:4])
+    hit = tuning.lookup(c.storage, n_tx, n_rx, n_s, n_f, c.workload.n_vox, _grid.detect(c.tensors["scan"]),
+                        int(c.workload.params["interp_type"]), torch.cuda.current_device(), "auto")
+    return hit or {}
 
 
 def make_acquisitions(channel, n: int) -> list:

@@ -7,7 +7,9 @@ grid.  None of them changes the
 result beyond summation order; every candidate is timed with CUDA events on the current
 stream over a few repetitions on the caller's own device-resident data, and the winner
 is cached per job shape and device in a JSON file (``MACH_B200_TUNING_CACHE``, default
-``~/.cache/mach_b200/tuning.json``).  mach itself has a fixed launch shape.
+``~/.cache/mach_b200/tuning.json``).  Automatic calls of :func:`mach_b200.experimental.beamform`
+and the serving engine's batch jobs look the cache up (:func:`lookup`) and run the tuned
+knobs when an entry exists.  mach itself has a fixed launch shape.
 """
 
 from __future__ import annotations
@@ -73,6 +75,44 @@ def candidates(storage: str, n_frames: int, grid: Any) -> list[dict]:
     return out
 
 
+_DEVICE_NAMES: dict[int, str] = {}
+_LOADED = False
+
+KNOBS = ("kernel", "tx_chunk", "window_rows", "lanes_per_voxel", "tile_fast", "frame_slots", "element_block",
+         "grid_shape")
+
+
+def resolve_delay(storage: str, delay: str) -> str:
+    """The delay mode a call runs with ("auto": mach's FP32 arithmetic for float32 / complex64
+    storage, split delays otherwise)."""
+    if delay == "auto":
+        return "reference" if storage in ("f32", "c64") else "split"
+    return delay
+
+
+def _device_name(index: int) -> str:
+    name = _DEVICE_NAMES.get(index)
+    if name is None:
+        import torch
+
+        name = _DEVICE_NAMES[index] = torch.cuda.get_device_name(index)
+    return name
+
+
+def lookup(storage, n_tx, n_rx, n_samples, n_frames, n_vox, grid, interp, device_index, delay) -> dict | None:
+    """Launch knobs the autotuner chose for this job shape, or None if it has not timed one.
+    Reads the cache file once per process; called by every automatic beamforming call."""
+    global _LOADED
+    key = _key(storage, n_tx, n_rx, n_samples, n_frames, n_vox, grid, interp, _device_name(device_index),
+               resolve_delay(storage, delay))
+    with _LOCK:
+        if key not in _MEMO and not _LOADED:
+            _MEMO.update({k: v for k, v in _load().items() if k not in _MEMO})
+            _LOADED = True
+        hit = _MEMO.get(key)
+    return _restore(hit) if hit is not None else None
+
+
 def _key(storage, n_tx, n_rx, n_samples, n_frames, n_vox, grid, interp, device_name, delay="auto") -> str:
     return (f"{device_name}|{storage}|tx{n_tx}|rx{n_rx}|s{n_samples}|f{n_frames}|v{n_vox}|g{grid}|i{int(interp)}"
             f"|d{delay}")
@@ -119,7 +159,7 @@ def tune(channel_data, rx_coords_m, scan_coords_m, tx_wave_arrivals_s, *, reps: 
     n_vox = int(scan_coords_m.shape[0])
     grid = _grid.detect(scan_coords_m)
     key = _key(storage, n_tx, n_rx, n_samples, n_frames, n_vox, grid, params.get("interp_type", 1),
-               torch.cuda.get_device_name(channel_data.device), params.get("delay", "auto"))
+               _device_name(channel_data.device.index or 0), resolve_delay(storage, params.get("delay", "auto")))
     if use_cache:
         with _LOCK:
             if key in _MEMO:

@@ -45,3 +45,20 @@ def test_staged_lanes_respect_storage_limits():
     # no lane count that leaves half the lanes idle
     lanes = {c["lanes_per_voxel"] for c in tuning.candidates("c64", 8, None) if c["kernel"] == "staged"}
     assert lanes == {4, 8}
+
+
+def test_lookup_reads_the_cache_written_by_the_tuner(tmp_path, monkeypatch):
+    """Automatic calls find the knobs the tuner stored for the same job shape, device and
+    delay mode (auto resolved as the call resolves it), and nothing for other shapes."""
+    monkeypatch.setenv("MACH_B200_TUNING_CACHE", str(tmp_path / "tuning.json"))
+    monkeypatch.setattr(tuning, "_MEMO", {})
+    monkeypatch.setattr(tuning, "_LOADED", False)
+    monkeypatch.setitem(tuning._DEVICE_NAMES, 0, "NVIDIA B200")
+    grid = (128, 128, 128)
+    key = tuning._key("i16", 9, 1024, 2048, 16, 128 ** 3, grid, 1, "NVIDIA B200", tuning.resolve_delay("i16", "auto"))
+    tuning._store(key, {"kernel": "lane_voxel", "element_block": 64, "ms": 70.0})
+    assert tuning.resolve_delay("i16", "auto") == "split" and tuning.resolve_delay("c64", "auto") == "reference"
+    hit = tuning.lookup("i16", 9, 1024, 2048, 16, 128 ** 3, grid, 1, 0, "split")
+    assert hit == {"kernel": "lane_voxel", "element_block": 64}
+    assert tuning.lookup("i16", 9, 1024, 2048, 16, 128 ** 3, grid, 1, 0, "reference") is None
+    assert tuning.lookup("i16", 9, 1024, 2048, 1, 128 ** 3, grid, 1, 0, "auto") is None
