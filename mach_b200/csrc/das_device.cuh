@@ -137,7 +137,6 @@ struct DasArgs {
     int32_t map_wlog;
     int64_t map_outer;
     int32_t frame_chunks;   // lane-voxel 8-frame chunks: CTA b takes tile b / frame_chunks, chunk b % frame_chunks
-    int32_t row32;          // 1: channel rows start on 32-byte boundaries (256-bit vector loads)
     int32_t e_begin;        // lane-voxel kernels: elements [e_begin, e_end) of this launch
     int32_t e_end;
     int32_t start_base;     // floor(-t0 * fs): samples before it belong to tau < 0

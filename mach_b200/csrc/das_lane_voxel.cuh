@@ -171,35 +171,34 @@ __device__ __forceinline__ void widen8<kI16>(uint2 r, float2* o) {
     widen8<kCI16>(r, o);
 }
 
-// Load the NF frames of one sample (NF * sizeof(T) is a multiple of 16 bytes).  row32: the
-// row starts on a 32-byte boundary, so rows of a multiple of 32 bytes are read with 256-bit
-// loads (each lane's request covers whole 32-byte sectors; measured on B200: Doppler complex64
-// in 8-frame chunks 5.7 -> 4.0 ms, FP16 3.45 -> 3.30 ms).
+// Load the NF frames of one sample (NF * sizeof(T) is a multiple of 16 bytes).  Rows of a
+// multiple of 32 bytes are read with 256-bit loads, so that each lane's request covers whole
+// 32-byte sectors (the planner only runs them on 32-byte aligned rows; measured on B200:
+// Doppler complex64 in 8-frame chunks 5.7 -> 4.0 ms, FP16 3.45 -> 3.30 ms); others with
+// 128-bit loads.
 template <int S, int NF>
-__device__ __forceinline__ void load_frames(const typename Storage<S>::T* p, float2* o, bool row32) {
+__device__ __forceinline__ void load_frames(const typename Storage<S>::T* p, float2* o) {
     constexpr int kBytes = NF * static_cast<int>(sizeof(typename Storage<S>::T));
     static_assert(kBytes % 16 == 0, "vector frames need 16-byte rows");
     constexpr int kPairsPer8 = FramePairs<S, NF>::kValue / (kBytes / 8);
     if constexpr (kBytes % 32 == 0) {
-        if (row32) {
 #pragma unroll
-            for (int i = 0; i < kBytes / 32; ++i) {
-                unsigned r[8];
-                asm("ld.global.nc.v8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
-                    : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
-                    : "l"(reinterpret_cast<const char*>(p) + 32 * i));
+        for (int i = 0; i < kBytes / 32; ++i) {
+            unsigned r[8];
+            asm("ld.global.nc.v8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+                : "l"(reinterpret_cast<const char*>(p) + 32 * i));
 #pragma unroll
-                for (int k = 0; k < 4; ++k) widen8<S>(make_uint2(r[2 * k], r[2 * k + 1]), o + (4 * i + k) * kPairsPer8);
-            }
-            return;
+            for (int k = 0; k < 4; ++k) widen8<S>(make_uint2(r[2 * k], r[2 * k + 1]), o + (4 * i + k) * kPairsPer8);
         }
-    }
-    const uint4* q = reinterpret_cast<const uint4*>(p);
+    } else {
+        const uint4* q = reinterpret_cast<const uint4*>(p);
 #pragma unroll
-    for (int i = 0; i < kBytes / 16; ++i) {
-        const uint4 r = __ldg(q + i);
-        widen8<S>(make_uint2(r.x, r.y), o + (2 * i) * kPairsPer8);
-        widen8<S>(make_uint2(r.z, r.w), o + (2 * i + 1) * kPairsPer8);
+        for (int i = 0; i < kBytes / 16; ++i) {
+            const uint4 r = __ldg(q + i);
+            widen8<S>(make_uint2(r.x, r.y), o + (2 * i) * kPairsPer8);
+            widen8<S>(make_uint2(r.z, r.w), o + (2 * i + 1) * kPairsPer8);
+        }
     }
 }
 
@@ -487,10 +486,10 @@ __device__ __forceinline__ void lane_voxel_tile(const DasArgs& a, int64_t tile, 
                         // Real frames in pairs: the interpolation weights folded into the
                         // apodisation weight, acc += (1 - t) w a + t w b in packed FP32x2.
                         float2 va[kAcc];
-                        load_frames<S, NF>(p, va, a.row32 != 0);
+                        load_frames<S, NF>(p, va);
                         if constexpr (INTERP == kLinear) {
                             float2 vb[kAcc];
-                            load_frames<S, NF>(p + tp.step * fstride, vb, a.row32 != 0);
+                            load_frames<S, NF>(p + tp.step * fstride, vb);
                             const float wb = __fmul_rn(tp.w0, cw);
                             const float wa = __fsub_rn(cw, wb);
 #pragma unroll
@@ -507,14 +506,14 @@ __device__ __forceinline__ void lane_voxel_tile(const DasArgs& a, int64_t tile, 
                     if constexpr (kVec) {
                         float2 va[kAcc], vb[kAcc], vc[kAcc];
                         if constexpr (INTERP == kNearest) {
-                            load_frames<S, NF>(p, va, a.row32 != 0);
+                            load_frames<S, NF>(p, va);
                         } else if constexpr (INTERP == kLinear) {
-                            load_frames<S, NF>(p, va, a.row32 != 0);
-                            load_frames<S, NF>(p + tp.step * fstride, vb, a.row32 != 0);
+                            load_frames<S, NF>(p, va);
+                            load_frames<S, NF>(p + tp.step * fstride, vb);
                         } else {
-                            load_frames<S, NF>(p - fstride, va, a.row32 != 0);
-                            load_frames<S, NF>(p, vb, a.row32 != 0);
-                            load_frames<S, NF>(p + fstride, vc, a.row32 != 0);
+                            load_frames<S, NF>(p - fstride, va);
+                            load_frames<S, NF>(p, vb);
+                            load_frames<S, NF>(p + fstride, vc);
                         }
 #pragma unroll
                         for (int q = 0; q < kAcc; ++q) {

@@ -368,9 +368,11 @@ Plan plan_launch(int storage, uint64_t n_vox, uint32_t n_frames, uint32_t n_tx, 
     // Longer ensembles in chunks of 8 frames (one CTA per chunk and tile) of the voxel-per-lane
     // kernel: rows of 8 frames must be 16-byte vectors and every sample row a multiple of 16
     // bytes.
+    // (8-frame rows of 32 or more bytes are read with 256-bit loads: 32-byte aligned channel data)
+    const uintptr_t align8 = (8u * esz) % 32u == 0 ? 32 : 16;
     const bool lane8_ok = n_frames > 16 && n_frames % 8 == 0 && (8u * esz) % 16u == 0 &&
                           (static_cast<uint64_t>(n_frames) * esz) % 16u == 0 &&
-                          (!channel_on_device || reinterpret_cast<uintptr_t>(channel) % 16 == 0);
+                          (!channel_on_device || reinterpret_cast<uintptr_t>(channel) % align8 == 0);
     // Measured on B200 (200-frame Doppler): for 4-byte complex storage (cf16, cbf16, ci16) the
     // 8-frame chunks beat the ensemble kernel (3.5 vs 5.5 ms); for complex64 and real storage
     // the ensemble kernel wins.
@@ -400,9 +402,9 @@ Plan plan_launch(int storage, uint64_t n_vox, uint32_t n_frames, uint32_t n_tx, 
     // Host channel data is staged into fresh (aligned) device buffers.
     const bool vec_ok =
         n_frames % static_cast<uint32_t>(vf) == 0 && (!channel_on_device || reinterpret_cast<uintptr_t>(channel) % 8 == 0);
-    // 16 frames per sample as 16-byte vectors: rows must be 16-byte multiples and aligned.
-    const bool lane16_ok = n_frames == 16 && (16u * esz) % 16u == 0 &&
-                           (!channel_on_device || reinterpret_cast<uintptr_t>(channel) % 16 == 0);
+    // 16 frames per sample (32 bytes or more) as 256-bit vectors: 32-byte aligned rows.
+    const bool lane16_ok = n_frames == 16 && (16u * esz) % 32u == 0 &&
+                           (!channel_on_device || reinterpret_cast<uintptr_t>(channel) % 32 == 0);
     if (kind == MACH_B200_KERNEL_AUTO) {
         kind = (n_frames <= 8 || lane16_ok) ? MACH_B200_KERNEL_LANE_VOXEL
                                             : (vec_ok ? MACH_B200_KERNEL_STAGED : MACH_B200_KERNEL_WARP);
@@ -641,9 +643,6 @@ int dispatch_split(int storage, DasArgs a, int interp, const Plan& plan, cudaStr
         b.n_tx = static_cast<int32_t>(launch_tx_count(split, total, k));
         b.channel = ch + static_cast<size_t>(t0) * static_cast<size_t>(per_tx) * esz;
         b.arrivals = a.arrivals + t0 * a.n_vox;
-        b.row32 = (reinterpret_cast<uintptr_t>(b.channel) % 32 == 0 && (static_cast<size_t>(a.n_frames) * esz) % 32 == 0)
-                      ? 1
-                      : 0;
         CUtensorMap map;
         std::memset(&map, 0, sizeof(map));
         if ((plan.staged || plan.ensemble) && plan.st.use_tma && b.n_tx > 0) {
@@ -1544,10 +1543,6 @@ int batch_run(mach_b200_batch* b, const mach_b200_job* jobs, uint32_t n_jobs, cu
                          j.f_number, j.rx_start_s, j.sampling_freq_hz, j.sound_speed_m_s, j.modulation_freq_hz,
                          j.tukey_alpha, j.channel_scale, cplx, j.flags);
         bj.a.channel = j.channel_data;
-        bj.a.row32 = (reinterpret_cast<uintptr_t>(j.channel_data) % 32 == 0 &&
-                      (static_cast<size_t>(j.n_frames) * storage_bytes(j.storage)) % 32 == 0)
-                         ? 1
-                         : 0;
         bj.a.arrivals = j.tx_wave_arrivals_s;
         bj.a.out = j.out;
         bj.a.n_tx = static_cast<int32_t>(need_channel ? j.n_tx : 0);
