@@ -85,6 +85,8 @@ def parse_args():
     p.add_argument("--also", default=None,
                    help="extra workload:storage lines measured in the same run (default with the default "
                         "workload: doppler:c64,doppler:cf16; 'none' for none)")
+    p.add_argument("--delay", choices=["reference", "split", "auto"], default="reference",
+                   help="delay arithmetic: mach's FP32 (default), FP64-split, or the library default per storage")
     p.add_argument("--no-tune", dest="tune", action="store_false",
                    help="skip the autotuner pass in warm-up (run the planner's automatic choice)")
     p.add_argument("--launch", default="",
@@ -231,9 +233,12 @@ def l2_peak_gbs() -> float | None:
     return best
 
 
-def roofline(w, storage, kernel_s, key) -> dict:
+def roofline(w, storage, kernel_s, key, sm_mhz=None) -> dict:
     """HBM roofline of the dominant kernel (algorithmic bytes / CUDA-event time) with the DRAM
-    and L2 bytes of its ncu capture beside it (L2 against the probed L2 read bandwidth)."""
+    and L2 bytes of its ncu capture beside it (L2 against the probed L2 read bandwidth), and
+    its instruction-issue floor: the capture's warp instructions per step at one warp
+    instruction per SM sub-partition per clock (4 per SM), at the SM clock sampled in this
+    run."""
     peak, peak_kind = measured_peak_hbm()
     alg = algorithmic_bytes(w, storage)
     achieved = alg / kernel_s / 1e9
@@ -254,6 +259,16 @@ def roofline(w, storage, kernel_s, key) -> dict:
         r["l2_peak_source"] = "mach_b200_probe_l2_read in this run (ld.global.cg over 32/64 MB)"
         if lts:
             r["l2_frac"] = r["l2_achieved"] / l2_peak
+    inst = prof.get("warp_inst")
+    if inst and sm_mhz:
+        n_sm = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+        floor_s = inst / (4.0 * n_sm * sm_mhz * 1e6)
+        r["issue"] = {"warp_inst_per_step": inst, "floor_ms": floor_s * 1e3, "frac": floor_s / kernel_s,
+                      "sm_mhz": sm_mhz, "sms": n_sm, "source": prof.get("inst_source", "")}
+    if prof.get("l1_wavefront_pct") is not None:
+        r["l1_wavefront_pct_of_peak"] = prof["l1_wavefront_pct"]
+    if prof.get("binding"):
+        r["binding_limit"] = prof["binding"]
     return r
 
 
@@ -308,8 +323,16 @@ def workload_config(name, w, storage, world) -> dict:
     }
 
 
+DELAY_CHOICE = "reference"
+
+
 def delay_mode(storage: str) -> str:
-    return "split" if storage in ("f16", "cf16", "bf16", "cbf16") else "reference"
+    """Delay arithmetic of the measured lines: mach's FP32 delays by default (the reference
+    kernel's own arithmetic); `--delay split` forms sample positions in FP64 split form, and
+    `--delay auto` takes the library's default (split for 16-bit floating-point storage)."""
+    if DELAY_CHOICE == "auto":
+        return "split" if storage in ("f16", "cf16", "bf16", "cbf16") else "reference"
+    return DELAY_CHOICE
 
 
 def parse_also(args) -> list[tuple[str, str | None]]:
@@ -430,7 +453,7 @@ def measure_ours(args, name, storage, world, rank, local, headline):
                    "tuned": bool(args.tune and not (headline and args.launch))},
     }
     kernel_s = statistics.mean(per_step) / 1e3
-    line["roofline"] = roofline(w, storage, kernel_s, f"{name}:{storage}")
+    line["roofline"] = roofline(w, storage, kernel_s, f"{name}:{storage}", sm_mhz=clock_info.get("sm_mhz"))
     line["clocks"] = clock_info
     if not args.no_e2e:
         line["e2e"] = run_e2e(args, w, storage, ch, world, local, dict(knobs, grid_shape=grid_shape or False))
@@ -1129,7 +1152,9 @@ def measure_reference(args, name, storage, world, headline):
 
 
 def main():
+    global DELAY_CHOICE
     args = parse_args()
+    DELAY_CHOICE = args.delay
     world, rank, local = dist_setup()
     try:
         if args.impl == "reference":

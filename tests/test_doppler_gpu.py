@@ -57,3 +57,22 @@ def test_power_accumulates_on_gpu_and_overwrites_on_cpu(cuda):
     with pytest.warns(UserWarning):
         doppler.power_doppler(*host, out_h, **p)
     assert H.rel_l2(out_h, once.cpu().numpy()) <= 1e-5
+
+
+@pytest.mark.parametrize("storage,kernel", [("c64", "auto"), ("c64", "ensemble"), ("cf16", "auto"),
+                                            ("ci16", "ensemble")])
+def test_power_vs_fp64_oracle(cuda, storage, kernel):
+    """The power image against sum |x|^2 of the FP64 oracle's frames on the same stored samples
+    (not against the library's own frames): -60 dB, the project's bar against the oracle."""
+    import torch
+
+    from mach_b200 import doppler
+
+    w = _workload(storage, 64, 1)
+    p = {k: w.params[k] for k in H.PARAM_KEYS}
+    got = doppler.power_doppler(*_args(w), channel_scale=w.channel_scale, kernel=kernel, **p)
+    torch.cuda.synchronize()
+    frames = H.oracle(w, storage=storage)
+    want = (np.abs(frames) ** 2).sum(axis=1)
+    assert want.max() > 0
+    assert H.nrms_db(got.cpu().numpy(), want) <= -60.0
