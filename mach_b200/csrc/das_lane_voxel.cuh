@@ -92,8 +92,9 @@ __device__ __forceinline__ void split_phasor(float cycles, float& sn, float& cs)
     __sincosf(__fmul_rn(__fsub_rn(cycles, whole), 6.28318530717958647f), &sn, &cs);
 }
 
-// Interpolated sample at `row[idx * stride]` (stride = frames), widened to FP32.
-template <int S, int INTERP>
+// Interpolated sample at `row[idx * stride]` (stride = frames), widened to FP32.  PACKED:
+// complex quadratic taps in packed FP32x2, the same operations and order as the scalar form.
+template <int S, int INTERP, bool PACKED = false>
 __device__ __forceinline__ float2 tap_value(const typename Storage<S>::T* p, const TapPosition& tp, int stride) {
     using ST = Storage<S>;
     if constexpr (INTERP == kNearest) {
@@ -109,6 +110,10 @@ __device__ __forceinline__ float2 tap_value(const typename Storage<S>::T* p, con
         const float2 a = ST::load(p - stride);
         const float2 b = ST::load(p);
         const float2 c = ST::load(p + stride);
+        if constexpr (PACKED && ST::kComplex) {
+            return __ffma2_rn(make_float2(tp.w2, tp.w2), c,
+                              __ffma2_rn(make_float2(tp.w0, tp.w0), a, __fmul2_rn(make_float2(tp.w1, tp.w1), b)));
+        }
         float2 r;
         r.x = __fmaf_rn(tp.w2, c.x, __fmaf_rn(tp.w0, a.x, __fmul_rn(tp.w1, b.x)));
         r.y = ST::kComplex ? __fmaf_rn(tp.w2, c.y, __fmaf_rn(tp.w0, a.y, __fmul_rn(tp.w1, b.y))) : 0.f;
@@ -284,6 +289,11 @@ __device__ __forceinline__ void lane_voxel_tile(const DasArgs& a, int64_t tile, 
     float2 acc[kAcc];
 #pragma unroll
     for (int f = 0; f < kAcc; ++f) acc[f] = make_float2(0.f, 0.f);
+    // One-frame complex jobs with FP32 delays: sum(c w x) and sum(s w x) in packed FP32x2; the
+    // rotation sum((c + i s) w x) = sum(c w x) + i sum(s w x) is applied once after the loops
+    // (compounding complex64 2.00 -> 1.91 ms on B200; with split delays it was slower).
+    constexpr bool kDeferRot = NF == 1 && kCplx && !SPLIT;
+    float2 acc_c = make_float2(0.f, 0.f), acc_s = make_float2(0.f, 0.f);
 
     const T* const channel = static_cast<const T*>(a.channel);
     const int row_len = a.n_samples * fstride;  // samples per (transmit, element) row
@@ -413,7 +423,7 @@ __device__ __forceinline__ void lane_voxel_tile(const DasArgs& a, int64_t tile, 
                                     tp.step = 0;
                                 }
                                 const int row_u = in ? row + u * tx_step : row;
-                                xv[u] = tap_value<S, INTERP>(channel + (row_u + tp.idx * n_frames), tp, n_frames);
+                                xv[u] = tap_value<S, INTERP, kDeferRot>(channel + (row_u + tp.idx * n_frames), tp, n_frames);
                                 cwv[u] = cw;
                                 swv[u] = sw;
                                 okv[u] = ok;
@@ -422,7 +432,13 @@ __device__ __forceinline__ void lane_voxel_tile(const DasArgs& a, int64_t tile, 
                             for (int u = 0; u < 2; ++u) {
                                 const float2 x = xv[u];
                                 float2 r;
-                                if constexpr (kCplx) {
+                                if constexpr (kDeferRot) {
+                                    if (okv[u]) {
+                                        acc_c = __ffma2_rn(make_float2(cwv[u], cwv[u]), x, acc_c);
+                                        acc_s = __ffma2_rn(make_float2(swv[u], swv[u]), x, acc_s);
+                                    }
+                                    continue;
+                                } else if constexpr (kCplx) {
                                     r.x = __fmaf_rn(x.x, cwv[u], __fmaf_rn(-x.y, swv[u], acc[0].x));
                                     r.y = __fmaf_rn(x.y, cwv[u], __fmaf_rn(x.x, swv[u], acc[0].y));
                                 } else {
@@ -554,6 +570,10 @@ __device__ __forceinline__ void lane_voxel_tile(const DasArgs& a, int64_t tile, 
         }
     }
 
+    if constexpr (kDeferRot) {
+        acc[0].x = __fadd_rn(acc[0].x, __fsub_rn(acc_c.x, acc_s.y));
+        acc[0].y = __fadd_rn(acc[0].y, __fadd_rn(acc_c.y, acc_s.x));
+    }
     if constexpr (CS > 1) {  // add the lanes' partial sums of each voxel
 #pragma unroll
         for (int off = 1; off < CS; off <<= 1) {
