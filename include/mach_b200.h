@@ -108,7 +108,7 @@ typedef struct mach_b200_options {
                                 device from tx_params, by one kernel into a temporary [n_tx][n_scan]
                                 device array (tx_wave_arrivals_s may then be NULL) */
     int32_t tile_fast;       /* lane-voxel kernels on a known grid: voxels a warp takes along the
-                                contiguous axis (2, 4, 8 or 16; the rest of its 32 along the next
+                                contiguous axis (1, 2, 4, 8 or 16; the rest of its 32 along the next
                                 axis), 0 = automatic */
     const double* tx_params; /* [n_tx][8]: origin xyz (m), unit direction (plane) or focus xyz (m)
                                 (spherical), time offset (s), unused.  The arrival is the distance of

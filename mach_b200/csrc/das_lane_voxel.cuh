@@ -207,6 +207,58 @@ __device__ __forceinline__ void load_frames(const typename Storage<S>::T* p, flo
     }
 }
 
+// Raw 32-bit words of the NF frames of one sample (NF * sizeof(T) bytes, a multiple of 16;
+// 256-bit loads when a multiple of 32, as load_frames).
+template <int S, int NF>
+__device__ __forceinline__ void load_words(const typename Storage<S>::T* p, unsigned* w) {
+    constexpr int kBytes = NF * static_cast<int>(sizeof(typename Storage<S>::T));
+    static_assert(kBytes % 16 == 0, "vector frames need 16-byte rows");
+    if constexpr (kBytes % 32 == 0) {
+#pragma unroll
+        for (int i = 0; i < kBytes / 32; ++i) {
+            unsigned* r = w + 8 * i;
+            asm("ld.global.nc.v8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+                : "l"(reinterpret_cast<const char*>(p) + 32 * i));
+        }
+    } else {
+        const uint4* q = reinterpret_cast<const uint4*>(p);
+#pragma unroll
+        for (int i = 0; i < kBytes / 16; ++i) {
+            const uint4 r = __ldg(q + i);
+            w[4 * i] = r.x;
+            w[4 * i + 1] = r.y;
+            w[4 * i + 2] = r.z;
+            w[4 * i + 3] = r.w;
+        }
+    }
+}
+
+// Linear interpolation a + t (b - a) of one complex FP16 / BF16 sample pair (I, Q in one
+// 32-bit word each for a and b), in FP32.  b - a is formed by the mixed-precision subtract
+// (16-bit operand widened exactly inside the instruction), so only a is converted: the
+// result is bit-identical to widening both and subtracting in FP32.
+template <int S>
+__device__ __forceinline__ float2 lerp_half_word(unsigned wa, unsigned wb, float t) {
+    float2 r;
+    if constexpr (S == kCF16) {
+        asm("{\n\t.reg .b16 al, ah, bl, bh;\n\t.reg .f32 fa, fb, da, db;\n\t"
+            "mov.b32 {al, ah}, %2;\n\tmov.b32 {bl, bh}, %3;\n\t"
+            "cvt.f32.f16 fa, al;\n\tcvt.f32.f16 fb, ah;\n\t"
+            "sub.rn.f32.f16 da, bl, fa;\n\tsub.rn.f32.f16 db, bh, fb;\n\t"
+            "fma.rn.f32 %0, %4, da, fa;\n\tfma.rn.f32 %1, %4, db, fb;\n\t}"
+            : "=f"(r.x), "=f"(r.y) : "r"(wa), "r"(wb), "f"(t));
+    } else {
+        asm("{\n\t.reg .b16 al, ah, bl, bh;\n\t.reg .f32 fa, fb, da, db;\n\t"
+            "mov.b32 {al, ah}, %2;\n\tmov.b32 {bl, bh}, %3;\n\t"
+            "cvt.f32.bf16 fa, al;\n\tcvt.f32.bf16 fb, ah;\n\t"
+            "sub.rn.f32.bf16 da, bl, fa;\n\tsub.rn.f32.bf16 db, bh, fb;\n\t"
+            "fma.rn.f32 %0, %4, da, fa;\n\tfma.rn.f32 %1, %4, db, fb;\n\t}"
+            : "=f"(r.x), "=f"(r.y) : "r"(wa), "r"(wb), "f"(t));
+    }
+    return r;
+}
+
 // Receive-path Tukey weight.  The weight only scales a sample, so fast intrinsics are used
 // (their ~1e-7 error is far inside the 1e-5 parity budget); the aperture decision itself is
 // the exact FP32 test of kernel.cu:461.
@@ -516,6 +568,18 @@ __device__ __forceinline__ void lane_voxel_tile(const DasArgs& a, int64_t tile, 
                         } else {
 #pragma unroll
                             for (int q = 0; q < kAcc; ++q) acc[q] = __ffma2_rn(make_float2(cw, cw), va[q], acc[q]);
+                        }
+                        continue;
+                    }
+                    if constexpr (kVec && kCplx && INTERP == kLinear && (S == kCF16 || S == kCBF16)) {
+                        unsigned wa[NF], wb[NF];  // one (I, Q) word per frame
+                        load_words<S, NF>(p, wa);
+                        load_words<S, NF>(p + tp.step * fstride, wb);
+#pragma unroll
+                        for (int q = 0; q < NF; ++q) {
+                            const float2 x = lerp_half_word<S>(wa[q], wb[q], tp.w0);
+                            acc[q].x = __fmaf_rn(x.x, cw, __fmaf_rn(-x.y, sw, acc[q].x));
+                            acc[q].y = __fmaf_rn(x.y, cw, __fmaf_rn(x.x, sw, acc[q].y));
                         }
                         continue;
                     }

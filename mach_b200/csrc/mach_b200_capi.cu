@@ -436,11 +436,12 @@ Plan plan_launch(int storage, uint64_t n_vox, uint32_t n_frames, uint32_t n_tx, 
         p.lp.grid = dim3(static_cast<unsigned>((n_vox + vpc - 1) / vpc), 1, 1);
         // On a known grid: CTA tiles of wf x (128 / wf) voxels, warps of wf x (32 / wf).
         // Automatic: 2 along the contiguous axis for 16 frames (rows of 32+ bytes), else 4.
-        const int wf = o.tile_fast == 2 || o.tile_fast == 4 || o.tile_fast == 8 || o.tile_fast == 16
+        const int wf = o.tile_fast == 1 || o.tile_fast == 2 || o.tile_fast == 4 || o.tile_fast == 8 ||
+                               o.tile_fast == 16
                            ? o.tile_fast
                            : (n_frames >= 16 ? 2 : 4);
         if (grid_matches(o, n_vox) && o.grid_shape[2] >= wf) {
-            const int lw = wf == 2 ? 1 : (wf == 4 ? 2 : (wf == 8 ? 3 : 4));
+            const int lw = wf == 1 ? 0 : (wf == 2 ? 1 : (wf == 4 ? 2 : (wf == 8 ? 3 : 4)));
             p.lp.map_fast = o.grid_shape[2];
             p.lp.map_wlog = lw;
             p.lp.map_outer = static_cast<int64_t>(n_vox / static_cast<uint64_t>(o.grid_shape[2]));
