@@ -12,6 +12,7 @@
 #include <mutex>
 #include <string>
 #include <vector>
+#include <vector>
 
 #include "das_launch.cuh"
 #include "das_split.h"
@@ -619,6 +620,18 @@ struct DeviceBuffer {
 
 // Launch transmits [0, a.n_tx) so that every launch's channel span stays below 2^31 samples
 // (32-bit offsets inside the kernels).  Later launches always accumulate.
+// Lane-voxel launches (which may run the elements in blocks, one launch each).
+bool lane_voxel_plan(const Plan& plan) {
+    return !plan.staged && !plan.ensemble && !plan.frame_lane &&
+           (plan.lp.kind == kKindLaneVoxel1 || plan.lp.kind == kKindLaneVoxelN || plan.lp.kind == kKindLaneVoxel16 ||
+            plan.lp.kind == kKindLaneVoxel8);
+}
+
+// Host channel data of a job that runs in element blocks is staged block by block.
+bool element_block_staging(const Plan& plan, uint32_t n_rx) {
+    return lane_voxel_plan(plan) && plan.lp.element_block > 0 && static_cast<uint32_t>(plan.lp.element_block) < n_rx;
+}
+
 int dispatch_split(int storage, DasArgs a, int interp, const Plan& plan, cudaStream_t st) {
     const size_t esz = storage_bytes(storage);
     const int64_t per_tx = static_cast<int64_t>(a.n_rx) * a.row_stride;
@@ -634,9 +647,7 @@ int dispatch_split(int storage, DasArgs a, int interp, const Plan& plan, cudaStr
     }
     // Lane-voxel kernels may run the elements in blocks, one launch each, so that a launch's
     // channel data stays in L2 while every CTA sweeps it.
-    const bool lane_voxel = !plan.staged && !plan.ensemble && !plan.frame_lane &&
-                            (plan.lp.kind == kKindLaneVoxel1 || plan.lp.kind == kKindLaneVoxelN ||
-                             plan.lp.kind == kKindLaneVoxel16 || plan.lp.kind == kKindLaneVoxel8);
+    const bool lane_voxel = lane_voxel_plan(plan);
     const int eblk = lane_voxel && plan.lp.element_block > 0 ? plan.lp.element_block : std::max(a.n_rx, 1);
     for (int64_t k = 0; k < split.n_launch; ++k) {
         const int64_t t0 = launch_first_tx(split, k);
@@ -878,6 +889,60 @@ int compound_impl(int32_t storage, const void* channel_data, const float* rx_coo
         a.n_tx = static_cast<int32_t>(n_tx);
         a.accumulate = overwrite ? 0 : 1;
         if ((rc = dispatch_split(storage, a, interp_type, plan, stream))) return rc;
+    } else if (r_ch != kOnDevice && element_block_staging(plan, n_rx) &&
+               split_transmits(static_cast<int64_t>(n_rx) * a.row_stride, n_tx).n_launch == 1) {
+        // Element blocks (the lane-voxel launches of a job far larger than L2): the channel
+        // data gets one device buffer, filled block by block on a side stream (one 2-D copy of
+        // the block's rows of every transmit), and each block's launch waits only for its own
+        // rows, so the copy of block b + 1 overlaps the gather of block b.
+        const int eblk = plan.lp.element_block;
+        const size_t row_bytes = static_cast<size_t>(n_samples) * n_frames * esz;
+        const int n_blk = static_cast<int>((n_rx + eblk - 1) / eblk);
+        StreamHolder copy;
+        std::vector<cudaEvent_t> block_ready(static_cast<size_t>(n_blk), nullptr);
+        struct EventList {
+            std::vector<cudaEvent_t>& ev;
+            ~EventList() {
+                for (auto e : ev)
+                    if (e) cudaEventDestroy(e);
+            }
+        } events{block_ready};
+        MACH_B200_CUDA_TRY(cudaStreamCreateWithFlags(&copy.s, cudaStreamNonBlocking));
+        for (auto& e : block_ready) MACH_B200_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        MACH_B200_CUDA_TRY(d_ch[0].alloc(tx_bytes * n_tx, stream));
+        if (r_arr != kOnDevice) MACH_B200_CUDA_TRY(d_arr[0].alloc(arr_bytes * n_tx, stream));
+        cudaEvent_t ready;  // the copy stream must not start before the buffers exist
+        MACH_B200_CUDA_TRY(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
+        cudaEventRecord(ready, stream);
+        cudaStreamWaitEvent(copy.s, ready, 0);
+        cudaEventDestroy(ready);
+        if (r_arr != kOnDevice) {
+            MACH_B200_CUDA_TRY(cudaMemcpyAsync(d_arr[0].ptr, tx_wave_arrivals_s, arr_bytes * n_tx,
+                                               cudaMemcpyHostToDevice, copy.s));
+            a.arrivals = static_cast<const float*>(d_arr[0].ptr);
+        } else {
+            a.arrivals = tx_wave_arrivals_s;
+        }
+        a.channel = d_ch[0].ptr;
+        a.n_tx = static_cast<int32_t>(n_tx);
+        const char* h_ch = static_cast<const char*>(channel_data);
+        char* d_base = static_cast<char*>(d_ch[0].ptr);
+        for (int k = 0; k < n_blk; ++k) {
+            const int e0 = k * eblk;
+            const int e1 = std::min<int>(static_cast<int>(n_rx), e0 + eblk);
+            MACH_B200_CUDA_TRY(cudaMemcpy2DAsync(d_base + row_bytes * e0, tx_bytes, h_ch + row_bytes * e0, tx_bytes,
+                                                 row_bytes * static_cast<size_t>(e1 - e0), n_tx,
+                                                 cudaMemcpyHostToDevice, copy.s));
+            MACH_B200_CUDA_TRY(cudaEventRecord(block_ready[k], copy.s));
+            MACH_B200_CUDA_TRY(cudaStreamWaitEvent(stream, block_ready[k], 0));
+            DasArgs b = a;
+            b.e_begin = e0;
+            b.e_end = e1;
+            b.accumulate = (k > 0 || !overwrite) ? 1 : 0;
+            CUtensorMap map;
+            std::memset(&map, 0, sizeof(map));
+            MACH_B200_CUDA_TRY(dispatch(storage, b, interp_type, plan, map, stream));
+        }
     } else {
         // Transmit chunks (>= 64 MB, at most 8 of them) copied on a side stream while the
         // previous chunk is gathered.
