@@ -120,6 +120,10 @@ typedef struct mach_b200_options {
                                 per block of elements, accumulating), so that a launch's channel data
                                 stays in L2; 0 = automatic (blocks of about 80 MB of channel data for
                                 16-frame jobs above 126 MB), -1 or >= n_rx = one launch */
+    int32_t tile_order;      /* voxel-per-lane kernels on a known grid: 1 = CTAs take the tiles at the far
+                                end of the contiguous axis first (the deepest first for a depth-fastest
+                                scan: widest aperture, most work, so a launch ends on light tiles),
+                                2 = grid order; 0 = automatic (1, except 16-frame jobs) */
 } mach_b200_options;
 
 /* Transmit models (mach_b200_options.tx_model). */

@@ -59,6 +59,7 @@ class Options(ctypes.Structure):
         ("tx_params", ctypes.c_void_p),
         ("frame_slots", ctypes.c_int32),
         ("element_block", ctypes.c_int32),
+        ("tile_order", ctypes.c_int32),
     ]
 
 
@@ -67,7 +68,7 @@ KERNELS = {"auto": 0, "lane_voxel": 1, "staged": 2, "warp": 3, "ensemble": 4, "f
 
 def make_options(flags: int = 0, grid_shape=None, kernel: str | int = 0, tx_chunk: int = 0, window_rows: int = 0,
                  lanes_per_voxel: int = 0, tile_fast: int = 0, frame_slots: int = 0,
-                 element_block: int = 0) -> Options:
+                 element_block: int = 0, tile_order: int = 0) -> Options:
     o = Options()
     o.struct_size = ctypes.sizeof(Options)
     o.flags = int(flags)
@@ -81,6 +82,7 @@ def make_options(flags: int = 0, grid_shape=None, kernel: str | int = 0, tx_chun
     o.tile_fast = int(tile_fast)
     o.frame_slots = int(frame_slots)
     o.element_block = int(element_block)
+    o.tile_order = int(tile_order)
     return o
 
 

@@ -136,6 +136,10 @@ struct DasArgs {
     int32_t map_fast;
     int32_t map_wlog;
     int64_t map_outer;
+    // tile_rev = 1: tiles in fast-axis-major order from the far end of the contiguous axis (the
+    // deepest first for a depth-fastest scan, whose wide apertures make them the heaviest), so the
+    // CTAs that start last take light tiles; 0: grid order (outer-major).
+    int32_t tile_rev;
     int32_t frame_chunks;   // lane-voxel 8-frame chunks: CTA b takes tile b / frame_chunks, chunk b % frame_chunks
     int32_t e_begin;        // lane-voxel kernels: elements [e_begin, e_end) of this launch
     int32_t e_end;

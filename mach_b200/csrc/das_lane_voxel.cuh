@@ -278,9 +278,19 @@ __device__ __forceinline__ int64_t lane_voxel_index(const DasArgs& a, int64_t ti
     if (a.map_fast <= 0) return tile * VPC + j;
     const int lw = a.map_wlog;
     const int64_t tiles_fast = (a.map_fast + (1 << lw) - 1) >> lw;
-    const int64_t to = tile / tiles_fast;
-    const int64_t o = to * (VPC >> lw) + (j >> lw);
-    const int64_t f = ((tile - to * tiles_fast) << lw) + (j & ((1 << lw) - 1));
+    const int64_t per_outer = VPC >> lw;  // outer-axis voxels of a tile
+    int64_t to, tf;                        // the tile's outer and fast-axis tile coordinates
+    if (a.tile_rev) {
+        const int64_t tiles_outer = (a.map_outer + per_outer - 1) / per_outer;
+        const int64_t q = tile / tiles_outer;
+        to = tile - q * tiles_outer;
+        tf = tiles_fast - 1 - q;
+    } else {
+        to = tile / tiles_fast;
+        tf = tile - to * tiles_fast;
+    }
+    const int64_t o = to * per_outer + (j >> lw);
+    const int64_t f = (tf << lw) + (j & ((1 << lw) - 1));
     return (o < a.map_outer && f < a.map_fast) ? o * a.map_fast + f : a.n_vox;
 }
 

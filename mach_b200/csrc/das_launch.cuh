@@ -35,6 +35,7 @@ struct LaunchPlan {
     int map_fast;       // lane-voxel kernels: grid tiling (DasArgs::map_*), 0 = linear tiles
     int map_wlog;
     int64_t map_outer;
+    int tile_rev;       // lane-voxel kernels on a grid: far end of the contiguous axis first (DasArgs::tile_rev)
     int frame_chunks;   // lane-voxel 8-frame chunks per tile (DasArgs::frame_chunks)
     int element_block;  // lane-voxel kernels: elements per launch (0 = all), so that one launch's
                         // channel data stays resident in L2

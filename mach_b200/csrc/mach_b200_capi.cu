@@ -445,6 +445,10 @@ Plan plan_launch(int storage, uint64_t n_vox, uint32_t n_frames, uint32_t n_tx, 
             const int lw = wf == 1 ? 0 : (wf == 2 ? 1 : (wf == 4 ? 2 : (wf == 8 ? 3 : 4)));
             p.lp.map_fast = o.grid_shape[2];
             p.lp.map_wlog = lw;
+            // Heaviest tiles first (measured on B200: compounding 1.90 -> 1.72 ms, Doppler
+            // complex64 4.06 -> 3.84 ms, FP16 2.75 -> 2.48 ms; 3-D 16 frames 67.3 -> 67.8 ms,
+            // so 16-frame jobs keep the grid order).
+            p.lp.tile_rev = o.tile_order == 1 ? 1 : (o.tile_order == 2 ? 0 : (n_frames == 16 ? 0 : 1));
             p.lp.map_outer = static_cast<int64_t>(n_vox / static_cast<uint64_t>(o.grid_shape[2]));
             const int64_t per_outer = vpc >> lw;
             const int64_t tiles = ((p.lp.map_outer + per_outer - 1) / per_outer) * ((p.lp.map_fast + wf - 1) / wf);
@@ -838,6 +842,7 @@ int compound_impl(int32_t storage, const void* channel_data, const float* rx_coo
     a.tx_chunk = plan.lp.tx_chunk;
     a.map_fast = plan.lp.map_fast;
     a.map_wlog = plan.lp.map_wlog;
+    a.tile_rev = plan.lp.tile_rev;
     a.map_outer = plan.lp.map_outer;
     a.frame_chunks = plan.lp.frame_chunks;
 
@@ -1618,6 +1623,7 @@ int batch_run(mach_b200_batch* b, const mach_b200_job* jobs, uint32_t n_jobs, cu
         bj.a.tx_chunk = p.lp.tx_chunk;
         bj.a.map_fast = p.lp.map_fast;
         bj.a.map_wlog = p.lp.map_wlog;
+        bj.a.tile_rev = p.lp.tile_rev;
         bj.a.map_outer = p.lp.map_outer;
         bj.a.frame_chunks = p.lp.frame_chunks;
         bj.st = p.st;

@@ -54,6 +54,7 @@ def beamform(
     tile_fast: int = 0,
     frame_slots: int = 0,
     element_block: int = 0,
+    tile_order: int = 0,
 ) -> Any:
     """Beamform and coherently compound ``n_transmits`` transmits.
 
@@ -69,8 +70,9 @@ def beamform(
         grid_shape: ``(slow, mid, fast)`` extents when ``scan_coords_m`` is a flattened grid
             (fast = contiguous axis); ``None`` detects it, ``False`` disables tiling by grid.
             Only the voxel-to-CTA assignment depends on it, never the result.
-        kernel, window_rows, lanes_per_voxel, tx_chunk, tile_fast, frame_slots, element_block: launch
-            tuning (see ``mach_b200_options`` in include/mach_b200.h); the autotuner sets them.
+        kernel, window_rows, lanes_per_voxel, tx_chunk, tile_fast, frame_slots, element_block,
+            tile_order: launch tuning (see ``mach_b200_options`` in include/mach_b200.h); the
+            autotuner sets them.
         delay: ``"reference"`` computes delays in FP32 exactly as mach does (bit-identical
             sample positions); ``"split"`` forms each sample position and phase in FP64 per
             receive path and per transmit as an integer base + FP32 fraction (more accurate,
@@ -88,7 +90,7 @@ def beamform(
                      channel_scale=channel_scale, sync=sync, grid_shape=grid_shape, kernel=kernel,
                      window_rows=window_rows, lanes_per_voxel=lanes_per_voxel, tx_chunk=tx_chunk, delay=delay,
                      power=False, tile_fast=tile_fast, frame_slots=frame_slots,
-                     element_block=element_block)
+                     element_block=element_block, tile_order=tile_order)
 
 
 def _tuned(storage, n_tx, n_rx, n_samples, n_frames, n_points, grid, interp_type, delay, channel_data):
@@ -107,7 +109,8 @@ def _tuned(storage, n_tx, n_rx, n_samples, n_frames, n_points, grid, interp_type
 
 def _compound(channel_data, rx_coords_m, scan_coords_m, tx_wave_arrivals_s, out, *, rx_start_s, sampling_freq_hz,
               f_number, sound_speed_m_s, modulation_freq_hz, tukey_alpha, interp_type, channel_scale, sync, grid_shape,
-              kernel, window_rows, lanes_per_voxel, tx_chunk, delay, power, tile_fast=0, frame_slots=0, element_block=0):
+              kernel, window_rows, lanes_per_voxel, tx_chunk, delay, power, tile_fast=0, frame_slots=0, element_block=0,
+              tile_order=0):
     """Shared body of :func:`beamform` and :func:`mach_b200.doppler.power_doppler` (``power``:
     ``out`` is the float32 ``[n_points]`` power image instead of the frames)."""
     xp = array_namespace(channel_data)
@@ -216,7 +219,8 @@ def _compound(channel_data, rx_coords_m, scan_coords_m, tx_wave_arrivals_s, out,
                 element_block = tuned.get("element_block", 0)
     options = _cuda_impl.make_options(
         flags, grid_shape=grid_shape or None, kernel=kernel, tx_chunk=tx_chunk, window_rows=window_rows,
-        lanes_per_voxel=lanes_per_voxel, tile_fast=tile_fast, frame_slots=frame_slots, element_block=element_block)
+        lanes_per_voxel=lanes_per_voxel, tile_fast=tile_fast, frame_slots=frame_slots, element_block=element_block,
+        tile_order=tile_order)
     if waves is not None:
         options.tx_model = waves.model
         options.tx_params = arr.ptr

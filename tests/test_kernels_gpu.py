@@ -126,15 +126,17 @@ def test_lane_voxel_sixteen_frames(cuda, storage, interp):
 @pytest.mark.parametrize("name,n_frames", [("compound", 1), ("volume3d", 16), ("volume3d", 3)])
 def test_lane_voxel_grid_tiles_are_bit_identical(cuda, name, n_frames):
     """The voxel-to-warp assignment on a grid (4 x 8, 2 x 16, ... neighbours, edge tiles
-    partly empty) changes which thread sums a voxel, never the sum."""
+    partly empty) and the order in which CTAs take the tiles change which thread sums a voxel,
+    never the sum."""
     if name == "compound":
         w = H.small("compound", n_x=37, n_z=45, n_tx=3)  # extents not multiples of the tiles
     else:
         w = H.small("volume3d", n_side=7, n_elem_side=8, n_frames=n_frames, n_samples=1400)
     base = _run(w, kernel="lane_voxel", grid_shape=False)
-    for tile_fast in (0, 1, 2, 4, 8, 16):
-        got = _run(w, kernel="lane_voxel", tile_fast=tile_fast)
-        np.testing.assert_array_equal(got, base)
+    for tile_order in (0, 1, 2):  # automatic, far end of the contiguous axis first, grid order
+        for tile_fast in (0, 1, 2, 4, 8, 16):
+            got = _run(w, kernel="lane_voxel", tile_fast=tile_fast, tile_order=tile_order)
+            np.testing.assert_array_equal(got, base)
     assert np.abs(base).max() > 0
 
 
@@ -171,6 +173,8 @@ def test_lane_voxel_frame_chunks(cuda, storage, n_frames):
     other = _run(w, kernel="warp")
     assert np.abs(chunks).max() > 0
     assert H.rel_l2(chunks, other) <= 2e-6
+    for tile_order in (1, 2):  # the order in which CTAs take the tiles never changes a sum
+        np.testing.assert_array_equal(_run(w, kernel="lane_voxel", tile_order=tile_order), chunks)
     assert H.nrms_db(chunks, H.oracle(w, storage=storage)) <= -60.0
     if storage in ("cf16", "cbf16", "ci16"):
         np.testing.assert_array_equal(_run(w), chunks)  # the automatic choice
