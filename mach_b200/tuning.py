@@ -42,7 +42,7 @@ def candidates(storage: str, n_frames: int, grid: Any) -> list[dict]:
         for tile_fast in ((2, 4) if grid else (0,)):
             out.append({"kernel": "lane_voxel", "tile_fast": tile_fast})
     if n_frames <= 8 or n_frames == 16:
-        for tx_chunk in (8, 16, 32):
+        for tx_chunk in (8, 16, 32, 40):
             for tile_fast in ((2, 4, 8) if grid else (0,)):
                 for lanes in ((1, 2, 4) if n_frames == 1 else (0,)):
                     out.append({"kernel": "lane_voxel", "tx_chunk": tx_chunk, "tile_fast": tile_fast,

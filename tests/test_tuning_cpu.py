@@ -32,6 +32,7 @@ def test_lane_voxel_knobs():
     one = [c for c in tuning.candidates("c64", 1, (1, 512, 512)) if c["kernel"] == "lane_voxel"]
     assert {c["lanes_per_voxel"] for c in one} == {1, 2, 4}
     assert {c["tile_fast"] for c in one} == {2, 4, 8}
+    assert {c["tx_chunk"] for c in one} == {8, 16, 32, 40}
     no_grid = [c for c in tuning.candidates("c64", 1, None) if c["kernel"] == "lane_voxel"]
     assert {c["tile_fast"] for c in no_grid} == {0}
 
