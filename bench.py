@@ -5,12 +5,13 @@ One step = one complete beamforming job of the chosen workload with every input 
 HBM.  The default workload is the largest single-GPU configuration: 3-D DAS, 9 diverging
 waves, 32 x 32 matrix array (1024 elements), 128^3 voxels, 2048 int16 RF samples x 16
 frames, linear interpolation, f# 1.0.  The same JSON line also carries, under "workloads",
-the Doppler ensemble (5 plane waves x 200 frames, 256^2, complex64 and FP16 IQ storage)
-measured the same way in the same process.  Prints ONE JSON line on rank 0.
+the Doppler ensemble (5 plane waves x 200 frames, 256^2, complex64 and FP16 IQ storage) and
+the 75-transmit compounding job measured the same way in the same process, and on one GPU,
+under "serving", the serving stream (`--workload serving`).  Prints ONE JSON line on rank 0.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                   [--workload compound|doppler|plain2d|volume3d|volume3d16|serving|rf2iq|ingest]
-                  [--storage c64|cf16|...] [--also doppler:c64,doppler:cf16 | --also none]
+                  [--storage c64|cf16|...] [--also doppler:c64,doppler:cf16,compound:c64 | --also none]
 
 rf2iq and ingest time the front end before the beamformer (RF -> IQ by the analytic signal,
 and the acquisition-order rearrange) in channel samples/s.
@@ -335,11 +336,28 @@ def delay_mode(storage: str) -> str:
     return DELAY_CHOICE
 
 
+def default_line(args) -> bool:
+    """The default run (no workload, frame or grid override): it also measures the Doppler and
+    compounding lines and, on one GPU, the serving stream."""
+    return args.workload == "volume3d16" and not args.frames and not args.side and args.also is None
+
+
+def with_serving(line: dict, runner, args, world, rank, local) -> dict:
+    """Attach the serving stream's line to the default line (one GPU only); a failure there is
+    recorded in the line instead of losing the headline."""
+    if not default_line(args) or world != 1:
+        return line
+    try:
+        line["serving"] = runner(args, world, rank, local)
+    except Exception as exc:  # noqa: BLE001 - reported in the JSON line
+        line["serving"] = {"error": f"{type(exc).__name__}: {exc}"[:300]}
+    return line
+
+
 def parse_also(args) -> list[tuple[str, str | None]]:
     spec = args.also
     if spec is None:
-        spec = "doppler:c64,doppler:cf16" if args.workload == "volume3d16" and not args.frames and not args.side \
-            else "none"
+        spec = "doppler:c64,doppler:cf16,compound:c64" if default_line(args) else "none"
     if spec.strip().lower() in ("", "none"):
         return []
     out = []
@@ -357,7 +375,7 @@ def run_ours(args, world, rank, local):
     if also:
         line["workloads"] = [measure_ours(args, name, storage, world, rank, local, headline=False)
                              for name, storage in also]
-    return line
+    return with_serving(line, run_serving, args, world, rank, local)
 
 
 def measure_ours(args, name, storage, world, rank, local, headline):
@@ -1058,7 +1076,7 @@ def run_reference(args, world, rank, local):
             names.append(name)
     if names:
         line["workloads"] = [measure_reference(args, name, None, world, headline=False) for name in names]
-    return line
+    return with_serving(line, run_serving_reference, args, world, rank, local)
 
 
 def measure_reference(args, name, storage, world, headline):
