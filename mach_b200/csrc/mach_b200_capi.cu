@@ -637,6 +637,17 @@ bool lane_voxel_plan(const Plan& plan) {
             plan.lp.kind == kKindLaneVoxel8);
 }
 
+// Whether a staging buffer of `bytes` leaves at least as much device memory free (else the
+// transmit-chunk staging, whose buffers are bounded, is used).
+bool fits_on_device(size_t bytes) {
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return bytes <= free_b / 2;
+}
+
 // Host channel data of a job that runs in element blocks is staged block by block.
 bool element_block_staging(const Plan& plan, uint32_t n_rx) {
     return lane_voxel_plan(plan) && plan.lp.element_block > 0 && static_cast<uint32_t>(plan.lp.element_block) < n_rx;
@@ -901,7 +912,8 @@ int compound_impl(int32_t storage, const void* channel_data, const float* rx_coo
         a.accumulate = overwrite ? 0 : 1;
         if ((rc = dispatch_split(storage, a, interp_type, plan, stream))) return rc;
     } else if (r_ch != kOnDevice && element_block_staging(plan, n_rx) &&
-               split_transmits(static_cast<int64_t>(n_rx) * a.row_stride, n_tx).n_launch == 1) {
+               split_transmits(static_cast<int64_t>(n_rx) * a.row_stride, n_tx).n_launch == 1 &&
+               fits_on_device(tx_bytes * n_tx)) {
         // Element blocks (the lane-voxel launches of a job far larger than L2): the channel
         // data gets one device buffer, filled block by block on a side stream (one 2-D copy of
         // the block's rows of every transmit), and each block's launch waits only for its own
